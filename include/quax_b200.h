@@ -1,0 +1,104 @@
+/*
+ * quax_b200.h -- C ABI of the B200-native two-electron integral library
+ * (libquax_b200.so).
+ *
+ * This replaces the ERI subset of the reference's pybind11 module
+ * `libint_interface` (quax/integrals/libint_interface.cc:2784-2807).  The reference
+ * keeps global state between initialize() and finalize(); here the same state lives
+ * in an opaque handle, so several molecules can coexist.  All arguments are plain
+ * pointers and sizes; no torch, pybind11 or JAX types cross this boundary.
+ *
+ * Conventions
+ *   - Coordinates are in bohr.  (The reference's initialize() reads an Angstrom
+ *     xyz file through Libint; the Python layer of this package does that parse.)
+ *   - Shells are Cartesian (Libint "standard" component order xx,xy,xz,yy,yz,zz,...)
+ *     with Libint normalisation; coefficients are passed raw, as tabulated, and
+ *     normalised by the library (the reference's BasisSet does the same).
+ *   - Dense outputs use the reference layout: ERI row-major i*n^3+j*n^2+k*n+l
+ *     (libint_interface.cc:571-585); first-derivative tensor (3N, n, n, n, n)
+ *     (libint_interface.cc:2626-2627, reshaped at quax/integrals/tei.py:33).
+ *   - Every entry point returns QX_OK (0) or a negative QX_E_* code; the message is
+ *     available from qx_last_error() on the calling thread.  Kernels never trap: a
+ *     failure inside a kernel sets a device error word that the entry point reads.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *     Work on device buffers is stream-ordered and asynchronous unless stated.
+ *   - `out_on_device` = 1: the pointer is device memory of the handle's device and
+ *     the call is asynchronous on `stream`.  0: the pointer is host memory; the
+ *     library stages through device memory and returns after the copy completes.
+ */
+#ifndef QUAX_B200_H
+#define QUAX_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QX_OK 0
+#define QX_E_INVALID (-1)     /* bad argument (sizes, NaN coordinates, exponents...) */
+#define QX_E_CUDA (-2)        /* CUDA runtime error */
+#define QX_E_UNSUPPORTED (-3) /* angular momentum / derivative order not compiled */
+#define QX_E_NOMEM (-4)       /* device allocation failed */
+#define QX_E_DEVICE (-5)      /* a kernel reported an error through the error word */
+
+/* Highest angular momentum per shell compiled into this build. */
+#define QX_MAX_L 2
+
+typedef struct qx_handle qx_handle;
+
+/* Thread-local message of the last failing call (never NULL). */
+const char *qx_last_error(void);
+
+/* Library build information: highest shell AM and derivative order compiled.
+ * Replaces the module attribute LIBINT2_MAX_DERIV_ORDER
+ * (libint_interface.cc:2806). */
+int qx_max_deriv_order(void);
+int qx_max_l(void);
+
+/* Replaces initialize(xyz, basis1..4, ints_tol) (libint_interface.cc:38-95) for
+ * the case bs1 == bs2 == bs3 == bs4 that the ERI path uses (quax/methods/ints.py:20).
+ *   natom, coords[3*natom]        geometry in bohr
+ *   nshell, shell_l[], shell_nprim[], shell_atom[]
+ *   exps[], coefs[]               primitives of all shells concatenated (shell order)
+ *   pure                          0 = Cartesian (the reference); 1 is reserved
+ *   ints_tol                      the reference's `threshold` (Schwarz tolerance)
+ * The handle is bound to the CUDA device current at the call; it computes the
+ * Schwarz table (libint_interface.cc:158-229) and the screened, class-sorted list of
+ * unique shell quartets on that device. */
+int qx_initialize(int natom, const double *coords, int nshell, const int *shell_l, const int *shell_nprim,
+                  const int *shell_atom, const double *exps, const double *coefs, int pure, double ints_tol,
+                  qx_handle **out);
+
+/* Replaces finalize() (libint_interface.cc:97-99). */
+int qx_finalize(qx_handle *h);
+
+/* Sizes of the handle: number of basis functions, atoms and shells. */
+int qx_nbf(const qx_handle *h);
+int qx_natom(const qx_handle *h);
+int qx_nshell(const qx_handle *h);
+
+/* Number of screened 8-fold-unique shell quartets (the throughput unit) and the
+ * number of doubles qx_eri_unique writes. */
+long long qx_unique_quartets(const qx_handle *h);
+long long qx_unique_size(const qx_handle *h);
+
+/* Schwarz table as the reference computes it (libint_interface.cc:158-229):
+ * K[s1*nshell+s2] = max |(f1 f2|f1 f2)| (not square-rooted), symmetric, host
+ * memory of nshell*nshell doubles; *kmax receives max K. Synchronous. */
+int qx_schwarz(qx_handle *h, double *K, double *kmax);
+
+/* Replaces compute_2e_int("eri", 0.) (libint_interface.cc:486-647): the dense
+ * Cartesian ERI tensor, n^4 doubles, with the reference's screening; elements of
+ * screened-out quartets are zero. */
+int qx_compute_2e_int(qx_handle *h, double *out, int out_on_device, void *stream);
+
+/* Every screened unique quartet's contracted Cartesian block, written
+ * class by class (canonical shell order within a quartet: higher AM first).  The
+ * order is documented by qx_unique_layout.  No counterpart in the reference (it only
+ * produces the dense tensor); this is the throughput path. Device memory only. */
+int qx_eri_unique(qx_handle *h, double *out_dev, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QUAX_B200_H */

@@ -1,0 +1,90 @@
+"""Build libquax_b200.so for sm_100a (in-tree, no JIT cache).
+
+Each CUDA translation unit is compiled by nvcc in parallel into
+quax_b200/_build/*.o; an object is rebuilt when its source or any header under
+csrc/ or include/ is newer.  The objects are linked into
+quax_b200/libquax_b200.so with the CUDA runtime linked statically, so the
+library does not depend on which libcudart the host process loaded first.
+"""
+from __future__ import annotations
+
+import glob
+import os
+import shutil
+import subprocess
+import sys
+from concurrent.futures import ThreadPoolExecutor
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+BUILD = os.path.join(PKG, "_build")
+LIB = os.path.join(PKG, "libquax_b200.so")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ARCH + [
+    "-lineinfo",
+    "-O3",
+    "-std=c++17",
+    "-Xcompiler",
+    "-fPIC",
+    "-I" + os.path.join(ROOT, "include"),
+    "-I" + CSRC,
+]
+
+
+def nvcc() -> str:
+    for cand in (os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "bin", "nvcc"), shutil.which("nvcc")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def sources():
+    return sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "gen", "*.cu")))
+
+
+def _headers_mtime() -> float:
+    hs = glob.glob(os.path.join(CSRC, "**", "*.cuh"), recursive=True) + glob.glob(os.path.join(ROOT, "include", "*.h"))
+    return max((os.path.getmtime(h) for h in hs), default=0.0)
+
+
+def _obj(src: str) -> str:
+    rel = os.path.relpath(src, CSRC).replace(os.sep, "_")
+    return os.path.join(BUILD, rel[:-3] + ".o")
+
+
+def _compile(src: str, hmt: float, verbose: bool):
+    obj = _obj(src)
+    if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(src), hmt):
+        return obj, False
+    cmd = [nvcc()] + NVCC_FLAGS + ["-c", src, "-o", obj]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed on {src}:\n{r.stdout}\n{r.stderr}")
+    return obj, True
+
+
+def build(verbose: bool = False, jobs: int | None = None) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    gen_hdr = os.path.join(CSRC, "gen", "eri_classes.cuh")
+    if not os.path.exists(gen_hdr) or os.path.getmtime(gen_hdr) < os.path.getmtime(os.path.join(CSRC, "gen_eri.py")):
+        subprocess.run([sys.executable, os.path.join(CSRC, "gen_eri.py")], check=True)
+    hmt = _headers_mtime()
+    srcs = sources()
+    with ThreadPoolExecutor(max_workers=jobs or os.cpu_count() or 4) as ex:
+        results = list(ex.map(lambda s: _compile(s, hmt, verbose), srcs))
+    objs = [o for o, _ in results]
+    rebuilt = any(b for _, b in results)
+    if rebuilt or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
+        cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    return LIB
+
+
+if __name__ == "__main__":
+    t = __import__("time").time()
+    print(build(verbose="-v" in sys.argv), f"{__import__('time').time() - t:.1f}s")

@@ -1,0 +1,4 @@
+// Generated by quax_b200/csrc/gen_eri.py -- do not edit by hand.
+// ERI kernels of class (11|11).
+#include "../qx_kernels.cuh"
+QX_DEFINE_LAUNCH(5, 1, 1, 1, 1)

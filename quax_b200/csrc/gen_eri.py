@@ -1,0 +1,342 @@
+#!/usr/bin/env python3
+"""Generator of the per-class Obara-Saika / Head-Gordon-Pople device code.
+
+Emits ``gen/eri_classes.cuh``: one ``EriCls<LA,LB,LC,LD>`` and one
+``DerCls<LA,LB,LC,LD>`` specialisation per canonical angular-momentum class
+(LA>=LB, LC>=LD, (LA,LB) >= (LC,LD) in pair-class order).  Every recurrence step
+is emitted as straight-line FP64 code over named scalars, pruned to the values
+the class actually needs, so nvcc sees SSA values rather than an indexed array.
+
+Method (published mathematics, written here from the papers):
+  * VRR  -- Obara & Saika, J. Chem. Phys. 84, 3963 (1986), eq. (39) restricted
+    to [e0|f0]^(m) (b = d = 0) as in Head-Gordon & Pople, J. Chem. Phys. 89,
+    5777 (1988):
+      [e+1_i,0|00]^(m) = PA_i[e0|00]^(m) + WP_i[e0|00]^(m+1)
+                       + e_i/(2z) ([e-1_i,0|00]^(m) - rho/z [e-1_i,0|00]^(m+1))
+      [e0|f+1_j,0]^(m) = QC_j[e0|f0]^(m) + WQ_j[e0|f0]^(m+1)
+                       + f_j/(2h) ([e0|f-1_j,0]^(m) - rho/h [e0|f-1_j,0]^(m+1))
+                       + e_j/(2(z+h)) [e-1_j,0|f0]^(m+1)
+  * HRR  -- Head-Gordon & Pople: (a,b+1_i| = (a+1_i,b| + AB_i (a,b|, and the ket
+    analogue, applied once per contracted quartet.
+  * First derivatives -- d/dA_i g_a = 2 alpha g_{a+1_i} - a_i g_{a-1_i}; the
+    2alpha / 2beta / 2gamma weights are folded into separate primitive
+    accumulators, the D-centre derivative follows from translational invariance.
+
+Run:  python gen_eri.py [LMAX]   (default LMAX=2)
+"""
+from __future__ import annotations
+
+import os
+import sys
+from typing import Dict, List, Tuple
+
+Trip = Tuple[int, int, int]
+
+
+def comps(l: int) -> List[Trip]:
+    out = []
+    for lx in range(l, -1, -1):
+        for ly in range(l - lx, -1, -1):
+            out.append((lx, ly, l - lx - ly))
+    return out
+
+
+def ncart(l):
+    return (l + 1) * (l + 2) // 2
+
+
+def hoff(l):
+    return l * (l + 1) * (l + 2) // 6
+
+
+def lidx(t: Trip) -> int:
+    k = t[1] + t[2]
+    return k * (k + 1) // 2 + t[2]
+
+
+def gidx(t: Trip) -> int:
+    return hoff(sum(t)) + lidx(t)
+
+
+def sh(t: Trip, i: int, s: int) -> Trip:
+    y = list(t)
+    y[i] += s
+    return tuple(y)
+
+
+def first_dir(t: Trip) -> int:
+    return 0 if t[0] > 0 else (1 if t[1] > 0 else 2)
+
+
+XYZ = "xyz"
+
+
+class Emitter:
+    def __init__(self, prefix: str):
+        self.lines: List[str] = []
+        self.n = 0
+        self.prefix = prefix
+
+    def new(self, expr: str) -> str:
+        name = f"{self.prefix}{self.n}"
+        self.n += 1
+        self.lines.append(f"const double {name} = {expr};")
+        return name
+
+
+class VRR:
+    """Demand-driven VRR DAG over (e, f, m); leaves pref*F_m held in Fp[m]."""
+
+    def __init__(self, em: Emitter):
+        self.em = em
+        self.memo: Dict[Tuple[Trip, Trip, int], str] = {}
+
+    def get(self, e: Trip, f: Trip, m: int) -> str:
+        key = (e, f, m)
+        if key in self.memo:
+            return self.memo[key]
+        if sum(e) == 0 and sum(f) == 0:
+            name = f"Fp[{m}]"
+        elif sum(f) == 0:
+            i = first_dir(e)
+            n = e[i]
+            em1 = sh(e, i, -1)
+            terms = [f"q.PA{XYZ[i]} * {self.get(em1, f, m)}", f"q.WP{XYZ[i]} * {self.get(em1, f, m + 1)}"]
+            if n >= 2:
+                em2 = sh(e, i, -2)
+                terms.append(
+                    f"{float(n - 1)!r} * q.oo2z * ({self.get(em2, f, m)} - q.roz * {self.get(em2, f, m + 1)})"
+                )
+            name = self.em.new(" + ".join(terms))
+        else:
+            j = first_dir(f)
+            nf = f[j]
+            fm1 = sh(f, j, -1)
+            terms = [f"q.QC{XYZ[j]} * {self.get(e, fm1, m)}", f"q.WQ{XYZ[j]} * {self.get(e, fm1, m + 1)}"]
+            if nf >= 2:
+                fm2 = sh(f, j, -2)
+                terms.append(
+                    f"{float(nf - 1)!r} * q.oo2e * ({self.get(e, fm2, m)} - q.roe * {self.get(e, fm2, m + 1)})"
+                )
+            if e[j] >= 1:
+                terms.append(f"{float(e[j])!r} * q.oo2ze * {self.get(sh(e, j, -1), fm1, m + 1)}")
+            name = self.em.new(" + ".join(terms))
+        self.memo[key] = name
+        return name
+
+
+class AccSpace:
+    """Accumulator layout: e in [elo, ehi], f in [flo, fhi] (global Cartesian index)."""
+
+    def __init__(self, name: str, elo, ehi, flo, fhi):
+        self.name = name
+        self.elo, self.ehi, self.flo, self.fhi = max(elo, 0), ehi, max(flo, 0), fhi
+        self.ne = hoff(self.ehi + 1) - hoff(self.elo)
+        self.nf = hoff(self.fhi + 1) - hoff(self.flo)
+        self.size = self.ne * self.nf
+
+    def index(self, e: Trip, f: Trip) -> int:
+        return (gidx(e) - hoff(self.elo)) * self.nf + (gidx(f) - hoff(self.flo))
+
+    def targets(self):
+        for le in range(self.elo, self.ehi + 1):
+            for e in comps(le):
+                for lf in range(self.flo, self.fhi + 1):
+                    for f in comps(lf):
+                        yield e, f
+
+
+class HRR:
+    """HRR DAG over one accumulator space: ket first (reduce d), then bra."""
+
+    def __init__(self, em: Emitter, acc: AccSpace):
+        self.em = em
+        self.acc = acc
+        self.memo: Dict[Tuple[Trip, Trip, Trip, Trip], str] = {}
+
+    def get(self, a: Trip, b: Trip, c: Trip, d: Trip) -> str:
+        key = (a, b, c, d)
+        if key in self.memo:
+            return self.memo[key]
+        if sum(d) > 0:
+            j = first_dir(d)
+            x = self.get(a, b, sh(c, j, 1), sh(d, j, -1))
+            y = self.get(a, b, c, sh(d, j, -1))
+            name = self.em.new(f"{x} + CD{XYZ[j]} * {y}")
+        elif sum(b) > 0:
+            i = first_dir(b)
+            x = self.get(sh(a, i, 1), sh(b, i, -1), c, d)
+            y = self.get(a, sh(b, i, -1), c, d)
+            name = self.em.new(f"{x} + AB{XYZ[i]} * {y}")
+        else:
+            name = f"{self.acc.name}[{self.acc.index(a, c)}]"
+        self.memo[key] = name
+        return name
+
+
+def gen_plain(la, lb, lc, ld) -> str:
+    lab, lcd = la + lb, lc + ld
+    S = lab + lcd
+    acc = AccSpace("acc", la, lab, lc, lcd)
+    out: List[str] = []
+    out.append(f"template <> struct EriCls<{la}, {lb}, {lc}, {ld}> {{")
+    out.append(f"  static constexpr int S = {S};")
+    out.append(f"  static constexpr int NACC = {acc.size};")
+    out.append(f"  static constexpr int NOUT = {ncart(la) * ncart(lb) * ncart(lc) * ncart(ld)};")
+    # VRR + accumulate
+    em = Emitter("v")
+    vr = VRR(em)
+    acc_lines = []
+    for e, f in acc.targets():
+        acc_lines.append(f"acc[{acc.index(e, f)}] += {vr.get(e, f, 0)};")
+    out.append("  template <class Q>")
+    out.append(
+        "  static __device__ __forceinline__ void vrr(double* __restrict__ acc, const double* __restrict__ Fp, const Q& q) {"
+    )
+    out += ["    " + ln for ln in em.lines]
+    out += ["    " + ln for ln in acc_lines]
+    out.append("  }")
+    # HRR
+    em2 = Emitter("h")
+    hr = HRR(em2, acc)
+    st = []
+    k = 0
+    for a in comps(la):
+        for b in comps(lb):
+            for c in comps(lc):
+                for d in comps(ld):
+                    st.append(f"out[{k}] = {hr.get(a, b, c, d)};")
+                    k += 1
+    out.append(
+        "  static __device__ __forceinline__ void hrr(const double* __restrict__ acc, double* __restrict__ out,"
+        " double ABx, double ABy, double ABz, double CDx, double CDy, double CDz) {"
+    )
+    out.append("    (void)ABx; (void)ABy; (void)ABz; (void)CDx; (void)CDy; (void)CDz;")
+    out += ["    " + ln for ln in em2.lines]
+    out += ["    " + ln for ln in st]
+    out.append("  }")
+    out.append("};")
+    return "\n".join(out)
+
+
+def gen_deriv(la, lb, lc, ld) -> str:
+    """First-derivative class: 4 accumulators (U, 2a*, 2b*, 2c*) and a hrr that
+    writes 9 blocks (A_xyz, B_xyz, C_xyz); D follows by invariance."""
+    lab, lcd = la + lb, lc + ld
+    S = lab + lcd + 1
+    U = AccSpace("U", la - 1, lab, lc - 1, lcd)
+    WA = AccSpace("WA", la + 1, lab + 1, lc, lcd)
+    WB = AccSpace("WB", la, lab + 1, lc, lcd)
+    WC = AccSpace("WC", la, lab, lc + 1, lcd + 1)
+    nout = ncart(la) * ncart(lb) * ncart(lc) * ncart(ld)
+    out: List[str] = []
+    out.append(f"template <> struct DerCls<{la}, {lb}, {lc}, {ld}> {{")
+    out.append(f"  static constexpr int S = {S};")
+    out.append(f"  static constexpr int NU = {U.size}, NA = {WA.size}, NB = {WB.size}, NC = {WC.size};")
+    out.append(f"  static constexpr int NOUT = {nout};")
+    em = Emitter("v")
+    vr = VRR(em)
+    acc_lines = []
+    # group by VRR value so each value is loaded once and feeds every set using it
+    uses: Dict[Tuple[Trip, Trip], List[str]] = {}
+    for sp, w in ((U, None), (WA, "a2"), (WB, "b2"), (WC, "c2")):
+        for e, f in sp.targets():
+            uses.setdefault((e, f), []).append((sp, w))
+    for (e, f), lst in uses.items():
+        v = vr.get(e, f, 0)
+        for sp, w in lst:
+            if w is None:
+                acc_lines.append(f"{sp.name}[{sp.index(e, f)}] += {v};")
+            else:
+                acc_lines.append(f"{sp.name}[{sp.index(e, f)}] = fma({w}, {v}, {sp.name}[{sp.index(e, f)}]);")
+    out.append("  template <class Q>")
+    out.append(
+        "  static __device__ __forceinline__ void vrr(double* __restrict__ U, double* __restrict__ WA,"
+        " double* __restrict__ WB, double* __restrict__ WC, const double* __restrict__ Fp, const Q& q,"
+        " double a2, double b2, double c2) {"
+    )
+    out += ["    " + ln for ln in em.lines]
+    out += ["    " + ln for ln in acc_lines]
+    out.append("  }")
+    # HRR: out[(3*centre + i) * NOUT + k]
+    em2 = Emitter("h")
+    hU, hA, hB, hC = HRR(em2, U), HRR(em2, WA), HRR(em2, WB), HRR(em2, WC)
+    st = []
+    k = 0
+    for a in comps(la):
+        for b in comps(lb):
+            for c in comps(lc):
+                for d in comps(ld):
+                    for i in range(3):
+                        tA = hA.get(sh(a, i, 1), b, c, d)
+                        if a[i] > 0:
+                            tA = f"{tA} - {float(a[i])!r} * {hU.get(sh(a, i, -1), b, c, d)}"
+                        tB = hB.get(a, sh(b, i, 1), c, d)
+                        if b[i] > 0:
+                            tB = f"{tB} - {float(b[i])!r} * {hU.get(a, sh(b, i, -1), c, d)}"
+                        tC = hC.get(a, b, sh(c, i, 1), d)
+                        if c[i] > 0:
+                            tC = f"{tC} - {float(c[i])!r} * {hU.get(a, b, sh(c, i, -1), d)}"
+                        st.append(f"out[{(0 + i) * nout + k}] = {tA};")
+                        st.append(f"out[{(3 + i) * nout + k}] = {tB};")
+                        st.append(f"out[{(6 + i) * nout + k}] = {tC};")
+                    k += 1
+    out.append(
+        "  static __device__ __forceinline__ void hrr(const double* __restrict__ U, const double* __restrict__ WA,"
+        " const double* __restrict__ WB, const double* __restrict__ WC, double* __restrict__ out,"
+        " double ABx, double ABy, double ABz, double CDx, double CDy, double CDz) {"
+    )
+    out.append("    (void)ABx; (void)ABy; (void)ABz; (void)CDx; (void)CDy; (void)CDz;")
+    out += ["    " + ln for ln in em2.lines]
+    out += ["    " + ln for ln in st]
+    out.append("  }")
+    out.append("};")
+    return "\n".join(out)
+
+
+def pair_classes(lmax):
+    return [(a, b) for a in range(lmax + 1) for b in range(a + 1)]
+
+
+def quartet_classes(lmax):
+    pc = pair_classes(lmax)
+    out = []
+    for i, (la, lb) in enumerate(pc):
+        for j, (lc, ld) in enumerate(pc[: i + 1]):
+            out.append((la, lb, lc, ld))
+    return out
+
+
+def main():
+    lmax = int(sys.argv[1]) if len(sys.argv) > 1 else 2
+    here = os.path.dirname(os.path.abspath(__file__))
+    os.makedirs(os.path.join(here, "gen"), exist_ok=True)
+    hdr = [
+        "// Generated by quax_b200/csrc/gen_eri.py -- do not edit by hand.",
+        f"// Canonical classes up to l = {lmax}.",
+        "#pragma once",
+        f"#define QX_GEN_LMAX {lmax}",
+        "template <int LA, int LB, int LC, int LD> struct EriCls;",
+        "template <int LA, int LB, int LC, int LD> struct DerCls;",
+    ]
+    qc = quartet_classes(lmax)
+    hdr.append("// X(class_id, LA, LB, LC, LD) for every canonical quartet class")
+    hdr.append("#define QX_FOR_EACH_CLASS(X) " + " ".join(f"X({i}, {a}, {b}, {c}, {d})" for i, (a, b, c, d) in enumerate(qc)))
+    hdr.append(f"#define QX_NUM_CLASSES {len(qc)}")
+    hdr.append(f"#define QX_NUM_PAIR_CLASSES {len(pair_classes(lmax))}")
+    body = [gen_plain(*c) for c in qc]
+    dbody = [gen_deriv(*c) for c in quartet_classes(lmax)]
+    with open(os.path.join(here, "gen", "eri_classes.cuh"), "w") as f:
+        f.write("\n".join(hdr) + "\n\n" + "\n\n".join(body) + "\n")
+    for i, (a, b, c, d) in enumerate(qc):
+        with open(os.path.join(here, "gen", f"k_eri_{i:02d}.cu"), "w") as f:
+            f.write("// Generated by quax_b200/csrc/gen_eri.py -- do not edit by hand.\n")
+            f.write(f"// ERI kernels of class ({a}{b}|{c}{d}).\n")
+            f.write('#include "../qx_kernels.cuh"\n')
+            f.write(f"QX_DEFINE_LAUNCH({i}, {a}, {b}, {c}, {d})\n")
+    with open(os.path.join(here, "gen", "der_classes.cuh"), "w") as f:
+        f.write("\n".join(hdr[:3] + ["#include \"eri_classes.cuh\""]) + "\n\n" + "\n\n".join(dbody) + "\n")
+
+
+if __name__ == "__main__":
+    main()

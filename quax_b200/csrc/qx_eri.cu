@@ -1,0 +1,448 @@
+// qx_eri.cu -- host side of libquax_b200.so and the ERI quartet kernels.
+//
+// Host responsibilities (what the reference's libint_interface.cc does around
+// Libint):
+//   * validate and normalise the shells (Libint convention);
+//   * build shell-pair / primitive-pair records and upload them;
+//   * Schwarz screening with the reference's semantics
+//     (quax/integrals/libint_interface.cc:158-229), evaluated on the GPU;
+//   * enumerate the screened 8-fold-unique quartets, bucket them by
+//     angular-momentum class and sort each bucket by primitive counts;
+//   * launch one kernel per class.
+// Device work: one thread per contracted shell quartet; the generated per-class
+// VRR runs once per primitive quartet into FP64 accumulators and the generated
+// HRR runs once per contracted quartet, followed by the output epilogue.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "quax_b200.h"
+#include "qx_kernels.cuh"
+
+using namespace qx;
+
+// ------------------------------------------------------------------ errors ----
+static thread_local std::string g_err = "no error";
+
+static int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define QX_CUDA(call)                                                                                  \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess) return fail(QX_E_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                                           __FILE__, __LINE__);                                        \
+    } while (0)
+
+extern "C" const char* qx_last_error(void) { return g_err.c_str(); }
+extern "C" int qx_max_l(void) { return QX_GEN_LMAX; }
+extern "C" int qx_max_deriv_order(void) { return 1; }
+
+static constexpr int pair_class(int l1, int l2) { return l1 * (l1 + 1) / 2 + l2; }
+static constexpr int quartet_class(int pb, int pk) { return pb * (pb + 1) / 2 + pk; }
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+#define QX_ERI_ENTRY(id, a, b, c, d) &qx_launch_eri_##id,
+static const EriLaunch g_eri_launch[QX_NUM_CLASSES] = {QX_FOR_EACH_CLASS(QX_ERI_ENTRY)};
+#define QX_NOUT_ENTRY(id, a, b, c, d) EriCls<a, b, c, d>::NOUT,
+static const int g_class_nout[QX_NUM_CLASSES] = {QX_FOR_EACH_CLASS(QX_NOUT_ENTRY)};
+
+// ------------------------------------------------------------------ Boys table --
+static void boys_table_host(std::vector<double>& tab) {
+    tab.assign((size_t)BOYS_NG * BOYS_NM, 0.0);
+    for (int g = 0; g < BOYS_NG; ++g) {
+        const double T = g / BOYS_INV_H;
+        double F[BOYS_NM];
+        const int M = BOYS_NM - 1;
+        if (T == 0.0) {
+            for (int m = 0; m <= M; ++m) F[m] = 1.0 / (2 * m + 1);
+        } else {
+            // series at the top order, then downward recursion
+            long double term = 1.0L / (2 * M + 1), sum = term;
+            for (int k = 1; k < 4000; ++k) {
+                term *= 2.0L * T / (2 * M + 2 * k + 1);
+                sum += term;
+                if (term < sum * 1e-21L) break;
+            }
+            const long double eT = expl(-(long double)T);
+            long double Fm = eT * sum;
+            F[M] = (double)Fm;
+            for (int m = M; m > 0; --m) {
+                Fm = (2.0L * T * Fm + eT) / (2 * m - 1);
+                F[m - 1] = (double)Fm;
+            }
+        }
+        for (int m = 0; m < BOYS_NM; ++m) tab[(size_t)g * BOYS_NM + m] = F[m];
+    }
+}
+
+// ------------------------------------------------------------------ handle ----
+struct ClassWork {
+    long long nq = 0;
+    int2* d_q = nullptr;
+    long long unique_base = 0;
+};
+
+struct qx_handle {
+    int device = 0;
+    int natom = 0, nshell = 0, nbf = 0, pure = 0;
+    double tol = 0.0;
+    std::vector<int> l, nprim, atom, poff, bf;
+    std::vector<double> coords, centers, alpha, coef;
+    // all shell pairs s1 >= s2 (reference order), canonical records
+    std::vector<PairInfo> pairs;
+    std::vector<int> pcls;
+    PrimPair* d_prims = nullptr;
+    PairInfo* d_pairs = nullptr;
+    double* d_boys = nullptr;
+    int* d_err = nullptr;
+    std::vector<double> K;  // nshell^2
+    double kmax = 0.0;
+    ClassWork work[QX_NUM_CLASSES];
+    long long nunique = 0, unique_size = 0;
+};
+
+static int pair_index(int s1, int s2) { return s1 * (s1 + 1) / 2 + s2; }  // s1 >= s2
+
+static void free_handle(qx_handle* h) {
+    if (!h) return;
+    cudaFree(h->d_prims);
+    cudaFree(h->d_pairs);
+    cudaFree(h->d_boys);
+    cudaFree(h->d_err);
+    for (auto& w : h->work) cudaFree(w.d_q);
+    delete h;
+}
+
+static double dfact(int n) {
+    double r = 1.0;
+    while (n > 1) { r *= n; n -= 2; }
+    return r;
+}
+
+static int run_class(qx_handle* h, int cls, int mode, const int2* d_q, long long nq, double* out, long long n,
+                     long long base, cudaStream_t s) {
+    EriArgs a;
+    a.quartets = d_q;
+    a.nq = nq;
+    a.pairs = h->d_pairs;
+    a.prims = h->d_prims;
+    a.boys = h->d_boys;
+    a.out = out;
+    a.n = n;
+    a.base = base;
+    a.err = h->d_err;
+    g_eri_launch[cls](a, mode, s);
+    QX_CUDA(cudaGetLastError());
+    return QX_OK;
+}
+
+extern "C" int qx_initialize(int natom, const double* coords, int nshell, const int* shell_l, const int* shell_nprim,
+                             const int* shell_atom, const double* exps, const double* coefs, int pure,
+                             double ints_tol, qx_handle** out) {
+    if (!out) return fail(QX_E_INVALID, "qx_initialize: out is NULL");
+    *out = nullptr;
+    if (natom <= 0 || nshell <= 0 || !coords || !shell_l || !shell_nprim || !shell_atom || !exps || !coefs)
+        return fail(QX_E_INVALID, "qx_initialize: empty geometry or shell list");
+    if (pure != 0) return fail(QX_E_UNSUPPORTED, "qx_initialize: only Cartesian shells (pure=0) are supported");
+    if (!(ints_tol > 0.0) || !std::isfinite(ints_tol)) return fail(QX_E_INVALID, "qx_initialize: ints_tol must be > 0");
+    for (int i = 0; i < 3 * natom; ++i)
+        if (!std::isfinite(coords[i])) return fail(QX_E_INVALID, "qx_initialize: non-finite coordinate %d", i);
+    qx_handle* h = new qx_handle();
+    cudaGetDevice(&h->device);
+    h->natom = natom;
+    h->nshell = nshell;
+    h->pure = pure;
+    h->tol = ints_tol;
+    h->coords.assign(coords, coords + 3 * natom);
+    int off = 0, bf = 0;
+    for (int s = 0; s < nshell; ++s) {
+        const int l = shell_l[s], k = shell_nprim[s], at = shell_atom[s];
+        if (l < 0 || l > QX_GEN_LMAX) {
+            free_handle(h);
+            return fail(QX_E_UNSUPPORTED, "qx_initialize: shell %d has l=%d (compiled max %d)", s, l, QX_GEN_LMAX);
+        }
+        if (k <= 0 || k > 64) {
+            free_handle(h);
+            return fail(QX_E_INVALID, "qx_initialize: shell %d has %d primitives (1..64 allowed)", s, k);
+        }
+        if (at < 0 || at >= natom) {
+            free_handle(h);
+            return fail(QX_E_INVALID, "qx_initialize: shell %d on atom %d of %d", s, at, natom);
+        }
+        h->l.push_back(l);
+        h->nprim.push_back(k);
+        h->atom.push_back(at);
+        h->poff.push_back(off);
+        h->bf.push_back(bf);
+        for (int c = 0; c < 3; ++c) h->centers.push_back(coords[3 * at + c]);
+        // Libint-convention normalisation
+        const double df = dfact(2 * l - 1);
+        std::vector<double> c(k);
+        for (int p = 0; p < k; ++p) {
+            const double a = exps[off + p];
+            if (!(a > 0.0) || !std::isfinite(a) || !std::isfinite(coefs[off + p])) {
+                free_handle(h);
+                return fail(QX_E_INVALID, "qx_initialize: shell %d primitive %d has exponent %g", s, p, a);
+            }
+            c[p] = coefs[off + p] * std::sqrt(std::pow(2.0, l) * std::pow(2.0 * a, l + 1.5) / (std::pow(M_PI, 1.5) * df));
+        }
+        double nrm = 0.0;
+        for (int p = 0; p < k; ++p)
+            for (int q = 0; q < k; ++q)
+                nrm += c[p] * c[q] * df * std::pow(M_PI, 1.5) / (std::pow(2.0, l) * std::pow(exps[off + p] + exps[off + q], l + 1.5));
+        if (!(nrm > 0.0)) {
+            free_handle(h);
+            return fail(QX_E_INVALID, "qx_initialize: shell %d has a degenerate contraction", s);
+        }
+        for (int p = 0; p < k; ++p) {
+            h->alpha.push_back(exps[off + p]);
+            h->coef.push_back(c[p] / std::sqrt(nrm));
+        }
+        off += k;
+        bf += ncart_h(l);
+    }
+    h->nbf = bf;
+    // pair records
+    std::vector<PrimPair> prims;
+    const double kfac = std::sqrt(2.0) * std::pow(M_PI, 1.25);
+    for (int s1 = 0; s1 < nshell; ++s1)
+        for (int s2 = 0; s2 <= s1; ++s2) {
+            int f = s1, g = s2;
+            if (h->l[s2] > h->l[s1]) std::swap(f, g);
+            PairInfo pi;
+            const double* A = &h->centers[3 * f];
+            const double* B = &h->centers[3 * g];
+            pi.Ax = A[0]; pi.Ay = A[1]; pi.Az = A[2];
+            pi.ABx = A[0] - B[0]; pi.ABy = A[1] - B[1]; pi.ABz = A[2] - B[2];
+            const double AB2 = pi.ABx * pi.ABx + pi.ABy * pi.ABy + pi.ABz * pi.ABz;
+            pi.prim_off = (int)prims.size();
+            pi.nprim = h->nprim[f] * h->nprim[g];
+            pi.bf1 = h->bf[f]; pi.bf2 = h->bf[g];
+            pi.s1 = f; pi.s2 = g;
+            pi.atom1 = h->atom[f]; pi.atom2 = h->atom[g];
+            pi.l1 = h->l[f]; pi.l2 = h->l[g];
+            for (int p = 0; p < h->nprim[f]; ++p)
+                for (int q = 0; q < h->nprim[g]; ++q) {
+                    const double a = h->alpha[h->poff[f] + p], b = h->alpha[h->poff[g] + q];
+                    const double ca = h->coef[h->poff[f] + p], cb = h->coef[h->poff[g] + q];
+                    PrimPair r;
+                    r.zeta = a + b;
+                    r.oo2z = 0.5 / r.zeta;
+                    r.Px = (a * A[0] + b * B[0]) / r.zeta;
+                    r.Py = (a * A[1] + b * B[1]) / r.zeta;
+                    r.Pz = (a * A[2] + b * B[2]) / r.zeta;
+                    r.PAx = r.Px - A[0]; r.PAy = r.Py - A[1]; r.PAz = r.Pz - A[2];
+                    r.K = kfac * ca * cb * std::exp(-a * b / r.zeta * AB2) / r.zeta;
+                    r.alpha = a;
+                    prims.push_back(r);
+                }
+            h->pairs.push_back(pi);
+            h->pcls.push_back(pair_class(pi.l1, pi.l2));
+        }
+    std::vector<double> boys;
+    boys_table_host(boys);
+    const int np = (int)h->pairs.size();
+#define QX_ALLOC(ptr, bytes)                                                          \
+    do {                                                                              \
+        if (cudaMalloc((void**)&(ptr), (bytes)) != cudaSuccess) {                     \
+            cudaGetLastError();                                                       \
+            free_handle(h);                                                           \
+            return fail(QX_E_NOMEM, "qx_initialize: cudaMalloc of %zu bytes failed", \
+                        (size_t)(bytes));                                             \
+        }                                                                             \
+    } while (0)
+    QX_ALLOC(h->d_prims, sizeof(PrimPair) * prims.size());
+    QX_ALLOC(h->d_pairs, sizeof(PairInfo) * np);
+    QX_ALLOC(h->d_boys, sizeof(double) * boys.size());
+    QX_ALLOC(h->d_err, sizeof(int));
+    cudaMemcpy(h->d_prims, prims.data(), sizeof(PrimPair) * prims.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(h->d_pairs, h->pairs.data(), sizeof(PairInfo) * np, cudaMemcpyHostToDevice);
+    cudaMemcpy(h->d_boys, boys.data(), sizeof(double) * boys.size(), cudaMemcpyHostToDevice);
+    cudaMemset(h->d_err, 0, sizeof(int));
+    // Schwarz: diagonal quartets (P|P) of every pair
+    {
+        std::vector<std::vector<int2>> diag(QX_NUM_PAIR_CLASSES);
+        for (int p = 0; p < np; ++p) diag[h->pcls[p]].push_back(make_int2(p, p));
+        double* d_kp = nullptr;
+        int2* d_dq = nullptr;
+        QX_ALLOC(d_kp, sizeof(double) * np);
+        QX_ALLOC(d_dq, sizeof(int2) * np);
+        long long o = 0;
+        for (int pc = 0; pc < QX_NUM_PAIR_CLASSES; ++pc) {
+            if (diag[pc].empty()) continue;
+            cudaMemcpy(d_dq + o, diag[pc].data(), sizeof(int2) * diag[pc].size(), cudaMemcpyHostToDevice);
+            int rc = run_class(h, quartet_class(pc, pc), MODE_SCHWARZ, d_dq + o, (long long)diag[pc].size(), d_kp, 0,
+                               0, 0);
+            if (rc) { cudaFree(d_kp); cudaFree(d_dq); free_handle(h); return rc; }
+            o += diag[pc].size();
+        }
+        std::vector<double> kp(np);
+        cudaError_t e = cudaMemcpy(kp.data(), d_kp, sizeof(double) * np, cudaMemcpyDeviceToHost);
+        cudaFree(d_kp);
+        cudaFree(d_dq);
+        if (e != cudaSuccess) {
+            free_handle(h);
+            return fail(QX_E_CUDA, "qx_initialize: Schwarz kernels failed: %s", cudaGetErrorString(e));
+        }
+        h->K.assign((size_t)nshell * nshell, 0.0);
+        for (int p = 0; p < np; ++p) {
+            const int s1 = h->pairs[p].s1, s2 = h->pairs[p].s2;
+            h->K[(size_t)s1 * nshell + s2] = h->K[(size_t)s2 * nshell + s1] = kp[p];
+            h->kmax = std::max(h->kmax, kp[p]);
+        }
+    }
+    // screened pair list (reference order s1 >= s2) and unique quartets
+    const double thr2 = ints_tol * ints_tol;
+    const double cut = thr2 / h->kmax;
+    std::vector<int> kept;
+    std::vector<double> kk;
+    for (int s1 = 0; s1 < nshell; ++s1)
+        for (int s2 = 0; s2 <= s1; ++s2)
+            if (h->K[(size_t)s1 * nshell + s2] >= cut) {
+                kept.push_back(pair_index(s1, s2));
+                kk.push_back(h->K[(size_t)s1 * nshell + s2]);
+            }
+    std::vector<std::vector<int2>> lists(QX_NUM_CLASSES);
+    for (size_t i = 0; i < kept.size(); ++i)
+        for (size_t j = 0; j <= i; ++j) {
+            if (kk[i] * kk[j] < thr2) continue;
+            int pb = kept[i], pk = kept[j];
+            if (h->pcls[pb] < h->pcls[pk]) std::swap(pb, pk);
+            lists[quartet_class(h->pcls[pb], h->pcls[pk])].push_back(make_int2(pb, pk));
+        }
+    long long base = 0;
+    for (int c = 0; c < QX_NUM_CLASSES; ++c) {
+        auto& L = lists[c];
+        // counting sort by (bra nprim, ket nprim): equal trip counts within a warp
+        std::vector<long long> cnt(64 * 64 + 1, 0);
+        auto key = [&](const int2& q) { return (h->pairs[q.x].nprim - 1) * 64 + (h->pairs[q.y].nprim - 1); };
+        for (auto& q : L) cnt[std::min(key(q), 64 * 64 - 1) + 1]++;
+        for (int k = 0; k < 64 * 64; ++k) cnt[k + 1] += cnt[k];
+        std::vector<int2> sorted(L.size());
+        for (auto& q : L) sorted[cnt[std::min(key(q), 64 * 64 - 1)]++] = q;
+        ClassWork& w = h->work[c];
+        w.nq = (long long)sorted.size();
+        w.unique_base = base;
+        base += w.nq * g_class_nout[c];
+        h->nunique += w.nq;
+        if (w.nq) {
+            QX_ALLOC(w.d_q, sizeof(int2) * w.nq);
+            cudaMemcpy(w.d_q, sorted.data(), sizeof(int2) * w.nq, cudaMemcpyHostToDevice);
+        }
+    }
+    h->unique_size = base;
+#undef QX_ALLOC
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        free_handle(h);
+        return fail(QX_E_CUDA, "qx_initialize: %s", cudaGetErrorString(e));
+    }
+    *out = h;
+    return QX_OK;
+}
+
+extern "C" int qx_finalize(qx_handle* h) {
+    if (!h) return fail(QX_E_INVALID, "qx_finalize: NULL handle");
+    DeviceGuard g(h->device);
+    free_handle(h);
+    return QX_OK;
+}
+
+extern "C" int qx_nbf(const qx_handle* h) { return h ? h->nbf : fail(QX_E_INVALID, "NULL handle"); }
+extern "C" int qx_natom(const qx_handle* h) { return h ? h->natom : fail(QX_E_INVALID, "NULL handle"); }
+extern "C" int qx_nshell(const qx_handle* h) { return h ? h->nshell : fail(QX_E_INVALID, "NULL handle"); }
+extern "C" long long qx_unique_quartets(const qx_handle* h) { return h ? h->nunique : -1; }
+extern "C" long long qx_unique_size(const qx_handle* h) { return h ? h->unique_size : -1; }
+
+extern "C" int qx_schwarz(qx_handle* h, double* K, double* kmax) {
+    if (!h || !K) return fail(QX_E_INVALID, "qx_schwarz: NULL argument");
+    std::memcpy(K, h->K.data(), sizeof(double) * h->K.size());
+    if (kmax) *kmax = h->kmax;
+    return QX_OK;
+}
+
+static int check_err_word(qx_handle* h, cudaStream_t s) {
+    int e = 0;
+    QX_CUDA(cudaMemcpyAsync(&e, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    QX_CUDA(cudaStreamSynchronize(s));
+    if (e) {
+        cudaMemsetAsync(h->d_err, 0, sizeof(int), s);
+        return fail(QX_E_DEVICE, "kernel error word 0x%x", e);
+    }
+    return QX_OK;
+}
+
+static int eri_dense_dev(qx_handle* h, double* out, cudaStream_t s) {
+    const long long n = h->nbf;
+    QX_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * n * n * n * n, s));
+    for (int c = 0; c < QX_NUM_CLASSES; ++c) {
+        const ClassWork& w = h->work[c];
+        if (!w.nq) continue;
+        int rc = run_class(h, c, MODE_DENSE, w.d_q, w.nq, out, n, 0, s);
+        if (rc) return rc;
+    }
+    return QX_OK;
+}
+
+extern "C" int qx_compute_2e_int(qx_handle* h, double* out, int out_on_device, void* stream) {
+    if (!h || !out) return fail(QX_E_INVALID, "qx_compute_2e_int: NULL argument");
+    DeviceGuard g(h->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const long long n = h->nbf;
+    const size_t bytes = sizeof(double) * (size_t)(n * n * n * n);
+    if (out_on_device) return eri_dense_dev(h, out, s);
+    double* d = nullptr;
+    if (cudaMalloc((void**)&d, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(QX_E_NOMEM, "qx_compute_2e_int: cannot stage %zu bytes on the device", bytes);
+    }
+    int rc = eri_dense_dev(h, d, s);
+    if (!rc) {
+        cudaError_t e = cudaMemcpyAsync(out, d, bytes, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) rc = fail(QX_E_CUDA, "qx_compute_2e_int: %s", cudaGetErrorString(e));
+    }
+    cudaFree(d);
+    if (!rc) rc = check_err_word(h, s);
+    return rc;
+}
+
+extern "C" int qx_eri_unique(qx_handle* h, double* out_dev, void* stream) {
+    if (!h || !out_dev) return fail(QX_E_INVALID, "qx_eri_unique: NULL argument");
+    DeviceGuard g(h->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    for (int c = 0; c < QX_NUM_CLASSES; ++c) {
+        const ClassWork& w = h->work[c];
+        if (!w.nq) continue;
+        int rc = run_class(h, c, MODE_UNIQUE, w.d_q, w.nq, out_dev, 0, w.unique_base, s);
+        if (rc) return rc;
+    }
+    return QX_OK;
+}

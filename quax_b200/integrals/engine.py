@@ -1,0 +1,117 @@
+"""Device-resident ERI engine: one C-ABI handle per molecule/basis.
+
+``EriEngine`` owns a ``qx_handle`` (shells, pair data, Schwarz table and the
+screened quartet lists live on the GPU) and returns torch tensors on that GPU.
+It is the object the reference-shaped ``libint_interface`` module and the
+``TEI`` primitives in this package are built on.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from ..basis import Basis
+from . import _lib
+
+
+def _stream_ptr(stream) -> int:
+    if stream is None:
+        return torch.cuda.current_stream().cuda_stream
+    return stream.cuda_stream
+
+
+class EriEngine:
+    def __init__(self, basis: Basis, ints_tol: float = 1.0e-14, device=None):
+        if basis.pure:
+            raise NotImplementedError("spherical shells are not supported by this build (Cartesian only)")
+        lib = _lib.load()
+        if not torch.cuda.is_available():
+            raise _lib.QuaxError("no CUDA device: the ERI engine has no CPU path")
+        self.device = torch.device(device if device is not None else f"cuda:{torch.cuda.current_device()}")
+        fl = basis.flat()
+        self.basis = basis
+        self.natom = basis.natom
+        coords = np.ascontiguousarray(basis.atom_coords().reshape(-1), dtype=np.float64)
+        self._keep = (coords, fl)
+        h = C.c_void_p()
+        with torch.cuda.device(self.device):
+            _lib.check(
+                lib.qx_initialize(
+                    basis.natom, _lib.dptr(coords), basis.nshell, _lib.iptr(fl["l"]), _lib.iptr(fl["nprim"]),
+                    _lib.iptr(fl["atom"]), _lib.dptr(fl["exps"]), _lib.dptr(fl["coefs"]), 0, float(ints_tol),
+                    C.byref(h),
+                ),
+                "qx_initialize",
+            )
+        self._h = h
+        self.nbf = lib.qx_nbf(h)
+        self.nshell = lib.qx_nshell(h)
+        self.ints_tol = ints_tol
+
+    # -- lifetime -------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _lib.load().qx_finalize(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise _lib.QuaxError("engine was finalized")
+        return self._h
+
+    # -- queries --------------------------------------------------------------
+    def unique_quartets(self) -> int:
+        return int(_lib.load().qx_unique_quartets(self.handle))
+
+    def unique_size(self) -> int:
+        return int(_lib.load().qx_unique_size(self.handle))
+
+    def schwarz(self):
+        K = np.empty((self.nshell, self.nshell))
+        kmax = C.c_double()
+        _lib.check(_lib.load().qx_schwarz(self.handle, _lib.dptr(K), C.byref(kmax)), "qx_schwarz")
+        return K, kmax.value
+
+    # -- integrals ------------------------------------------------------------
+    def eri(self, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+        """Dense (n,n,n,n) FP64 ERI tensor on the device (reference layout)."""
+        n = self.nbf
+        if out is None:
+            out = torch.empty((n, n, n, n), dtype=torch.float64, device=self.device)
+        assert out.is_contiguous() and out.dtype == torch.float64 and out.numel() == n**4
+        with torch.cuda.device(self.device):
+            _lib.check(
+                _lib.load().qx_compute_2e_int(self.handle, C.c_void_p(out.data_ptr()), 1, C.c_void_p(_stream_ptr(stream))),
+                "qx_compute_2e_int",
+            )
+        return out
+
+    def eri_host(self) -> np.ndarray:
+        """Dense tensor returned in host memory (the reference's return convention)."""
+        n = self.nbf
+        out = np.empty(n**4)
+        with torch.cuda.device(self.device):
+            _lib.check(
+                _lib.load().qx_compute_2e_int(self.handle, C.c_void_p(out.ctypes.data), 0, C.c_void_p(0)),
+                "qx_compute_2e_int",
+            )
+        return out
+
+    def eri_unique(self, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+        if out is None:
+            out = torch.empty(self.unique_size(), dtype=torch.float64, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.check(
+                _lib.load().qx_eri_unique(self.handle, C.c_void_p(out.data_ptr()), C.c_void_p(_stream_ptr(stream))),
+                "qx_eri_unique",
+            )
+        return out
