@@ -13,6 +13,7 @@ import os
 import shutil
 import subprocess
 import sys
+import time
 from concurrent.futures import ThreadPoolExecutor
 
 PKG = os.path.dirname(os.path.abspath(__file__))
@@ -58,9 +59,10 @@ def _compile(src: str, hmt: float, verbose: bool):
     if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(src), hmt):
         return obj, False
     cmd = [nvcc()] + NVCC_FLAGS + ["-c", src, "-o", obj]
-    if verbose:
-        print(" ".join(cmd), flush=True)
+    t0 = time.time()
     r = subprocess.run(cmd, capture_output=True, text=True)
+    if verbose:
+        print(f"{time.time() - t0:7.1f}s  {os.path.basename(src)}", flush=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc failed on {src}:\n{r.stdout}\n{r.stderr}")
     return obj, True
@@ -86,5 +88,5 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
 
 
 if __name__ == "__main__":
-    t = __import__("time").time()
-    print(build(verbose="-v" in sys.argv), f"{__import__('time').time() - t:.1f}s")
+    t = time.time()
+    print(build(verbose="-v" in sys.argv), f"{time.time() - t:.1f}s")

@@ -169,7 +169,7 @@ class HRR:
             y = self.get(a, sh(b, i, -1), c, d)
             name = self.em.new(f"{x} + AB{XYZ[i]} * {y}")
         else:
-            name = f"{self.acc.name}[{self.acc.index(a, c)}]"
+            name = f"{self.acc.name}({self.acc.index(a, c)})"
         self.memo[key] = name
         return name
 
@@ -186,34 +186,34 @@ def gen_plain(la, lb, lc, ld) -> str:
     # VRR + accumulate
     em = Emitter("v")
     vr = VRR(em)
-    acc_lines = []
-    for e, f in acc.targets():
-        acc_lines.append(f"acc[{acc.index(e, f)}] += {vr.get(e, f, 0)};")
-    out.append("  template <class Q>")
+    # highest bra AM first: measured to give the smallest peak of live values
+    for e, f in reversed(list(acc.targets())):
+        v = vr.get(e, f, 0)
+        em.lines.append(f"acc({acc.index(e, f)}) += {v};")
+    out.append("  template <class Acc, class Q>")
     out.append(
-        "  static __device__ __forceinline__ void vrr(double* __restrict__ acc, const double* __restrict__ Fp, const Q& q) {"
+        "  static __device__ __forceinline__ void vrr(Acc& acc, const double* __restrict__ Fp, const Q& q) {"
     )
     out += ["    " + ln for ln in em.lines]
-    out += ["    " + ln for ln in acc_lines]
     out.append("  }")
-    # HRR
+    # HRR (each output stored as soon as it is formed)
     em2 = Emitter("h")
     hr = HRR(em2, acc)
-    st = []
     k = 0
     for a in comps(la):
         for b in comps(lb):
             for c in comps(lc):
                 for d in comps(ld):
-                    st.append(f"out[{k}] = {hr.get(a, b, c, d)};")
+                    v = hr.get(a, b, c, d)
+                    em2.lines.append(f"st({k}, {v});")
                     k += 1
+    out.append("  template <class Acc, class St>")
     out.append(
-        "  static __device__ __forceinline__ void hrr(const double* __restrict__ acc, double* __restrict__ out,"
+        "  static __device__ __forceinline__ void hrr(Acc& acc, St& st,"
         " double ABx, double ABy, double ABz, double CDx, double CDy, double CDz) {"
     )
     out.append("    (void)ABx; (void)ABy; (void)ABz; (void)CDx; (void)CDy; (void)CDz;")
     out += ["    " + ln for ln in em2.lines]
-    out += ["    " + ln for ln in st]
     out.append("  }")
     out.append("};")
     return "\n".join(out)
@@ -294,6 +294,223 @@ def gen_deriv(la, lb, lc, ld) -> str:
     return "\n".join(out)
 
 
+# ----------------------------------------------------------------------------------
+# Table-driven programs for the warp-cooperative engine (large classes).
+# ----------------------------------------------------------------------------------
+# VRR node (uint4): x = dst | s1<<16, y = s2 | s3<<16, z = s4 | s5<<16,
+#                   w = side | dir<<1 | k<<3 | ne<<8
+#   V[dst] = c1[side,dir] V[s1] + c2[side,dir] V[s2] + k half[side] (V[s3] - ro[side] V[s4])
+#            + ne oo2ze V[s5]
+# slots 0..S hold pref*F_m, slot S+1 holds 0.
+# HRR node (uint2): x = dst | s1<<16, y = s2 | side<<16 | dir<<17 ;  V[dst] = V[s1] + g[side,dir] V[s2]
+# HRR leaves are the accumulators (slot = accumulator index).
+COOP_CLASSES = {(2, 1, 2, 1), (2, 2, 1, 1), (2, 2, 2, 1), (2, 2, 2, 2)}
+
+
+class VRRDag:
+    def __init__(self, S):
+        self.S = S
+        self.ZERO = S + 1
+        self.slot = {}
+        self.nodes = []  # (dst, s1, s2, s3, s4, s5, side, dir, k, ne, level)
+        self.level = {}
+
+    def get(self, e, f, m):
+        key = (e, f, m)
+        if key in self.slot:
+            return self.slot[key]
+        if sum(e) == 0 and sum(f) == 0:
+            return m
+        Z = self.ZERO
+        if sum(f) == 0:
+            i = first_dir(e)
+            n = e[i]
+            s1 = self.get(sh(e, i, -1), f, m)
+            s2 = self.get(sh(e, i, -1), f, m + 1)
+            s3 = self.get(sh(e, i, -2), f, m) if n >= 2 else Z
+            s4 = self.get(sh(e, i, -2), f, m + 1) if n >= 2 else Z
+            ops = (s1, s2, s3, s4, Z)
+            side, d, k, ne = 0, i, max(n - 1, 0), 0
+        else:
+            j = first_dir(f)
+            nf = f[j]
+            s1 = self.get(e, sh(f, j, -1), m)
+            s2 = self.get(e, sh(f, j, -1), m + 1)
+            s3 = self.get(e, sh(f, j, -2), m) if nf >= 2 else Z
+            s4 = self.get(e, sh(f, j, -2), m + 1) if nf >= 2 else Z
+            s5 = self.get(sh(e, j, -1), sh(f, j, -1), m + 1) if e[j] >= 1 else Z
+            ops = (s1, s2, s3, s4, s5)
+            side, d, k, ne = 1, j, max(nf - 1, 0), e[j]
+        lvl = 1 + max(self.level.get(o, 0) for o in ops)
+        dst = self.S + 2 + len(self.nodes)
+        self.nodes.append((dst,) + ops + (side, d, k, ne, lvl))
+        self.level[dst] = lvl
+        self.slot[key] = dst
+        return dst
+
+
+class HRRDag:
+    def __init__(self, acc):
+        self.acc = acc
+        self.slot = {}
+        self.nodes = []  # (dst, s1, s2, side, dir, level)
+        self.level = {}
+        self.next = acc.size
+
+    def get(self, a, b, c, d):
+        key = (a, b, c, d)
+        if key in self.slot:
+            return self.slot[key]
+        if sum(d) > 0:
+            j = first_dir(d)
+            s1 = self.get(a, b, sh(c, j, 1), sh(d, j, -1))
+            s2 = self.get(a, b, c, sh(d, j, -1))
+            side, dr = 1, j
+        elif sum(b) > 0:
+            i = first_dir(b)
+            s1 = self.get(sh(a, i, 1), sh(b, i, -1), c, d)
+            s2 = self.get(a, sh(b, i, -1), c, d)
+            side, dr = 0, i
+        else:
+            r = self.acc.index(a, c)
+            self.slot[key] = r
+            return r
+        lvl = 1 + max(self.level.get(s1, 0), self.level.get(s2, 0))
+        dst = self.next
+        self.next += 1
+        self.nodes.append((dst, s1, s2, side, dr, lvl))
+        self.level[dst] = lvl
+        self.slot[key] = dst
+        return dst
+
+
+def _realloc(simple, nodes, pinned, nfixed, kind):
+    """Reassign slots so a slot is reused once every reader sits in an earlier
+    level (nodes of one level run concurrently).  Fixed slots [0, nfixed) hold
+    the leaves; pinned slots are read after the last level."""
+    last = {}
+    for dst, ops, lvl in simple:
+        for o in ops:
+            last[o] = max(last.get(o, 0), lvl)
+    INF = 1 << 30
+    for p in pinned:
+        last[p] = INF
+    levels = sorted(set(l for _, _, l in simple))
+    remap = {i: i for i in range(nfixed)}
+    free = []
+    nxt = nfixed
+    by_level = {}
+    for dst, ops, lvl in simple:
+        by_level.setdefault(lvl, []).append(dst)
+    released = set()
+    for L in levels:
+        # release slots whose readers all precede level L
+        for old_slot, lu in list(last.items()):
+            if lu < L and old_slot in remap and old_slot not in released:
+                released.add(old_slot)
+                free.append(remap[old_slot])
+        for dst in by_level[L]:
+            if free:
+                remap[dst] = free.pop()
+            else:
+                remap[dst] = nxt
+                nxt += 1
+    out = []
+    for n in nodes:
+        if kind == "v":
+            dst, s1, s2, s3, s4, s5 = n[:6]
+            out.append((remap[dst], remap.get(s1, s1), remap.get(s2, s2), remap.get(s3, s3), remap.get(s4, s4),
+                        remap.get(s5, s5)) + tuple(n[6:]))
+        else:
+            dst, s1, s2 = n[:3]
+            out.append((remap[dst], remap.get(s1, s1), remap.get(s2, s2)) + tuple(n[3:]))
+    return out, [remap.get(p, p) for p in pinned], max(nxt, nfixed)
+
+
+def coop_program(la, lb, lc, ld):
+    S = la + lb + lc + ld
+    acc = AccSpace("acc", la, la + lb, lc, lc + ld)
+    vd = VRRDag(S)
+    targets = [vd.get(e, f, 0) for e, f in acc.targets()]
+    vnodes = sorted(vd.nodes, key=lambda n: n[-1])
+    vlev = []
+    for lv in range(1, max(n[-1] for n in vnodes) + 1):
+        vlev.append(sum(1 for n in vnodes if n[-1] < lv))
+    vlev.append(len(vnodes))
+    hd = HRRDag(acc)
+    outs = []
+    for a in comps(la):
+        for b in comps(lb):
+            for c in comps(lc):
+                for d in comps(ld):
+                    outs.append(hd.get(a, b, c, d))
+    hnodes = sorted(hd.nodes, key=lambda n: n[-1])
+    hlev = []
+    if hnodes:
+        for lv in range(1, max(n[-1] for n in hnodes) + 1):
+            hlev.append(sum(1 for n in hnodes if n[-1] < lv))
+    hlev.append(len(hnodes))
+    # liveness-based slot reuse (targets / outputs stay pinned to the end)
+    vnodes, targets, vslots = _realloc([(n[0], n[1:6], n[-1]) for n in vnodes], vnodes, targets, S + 2, "v")
+    hnodes, outs, hslots = _realloc([(n[0], n[1:3], n[-1]) for n in hnodes], hnodes, outs, acc.size, "h")
+    return dict(S=S, vnodes=vnodes, vlev=vlev, targets=targets, hnodes=hnodes, hlev=hlev, outs=outs,
+                vslots=vslots, hslots=hslots, nacc=acc.size)
+
+
+def gen_coop(classes):
+    lines = ["// Generated by quax_b200/csrc/gen_eri.py -- do not edit by hand.",
+             "// Programs of the warp-cooperative engine (large angular-momentum classes).",
+             "#pragma once", "#include <stdint.h>", ""]
+    vn, vl, tg, hn, hl, ou = [], [], [], [], [], []
+    descs = []
+    for cid, (la, lb, lc, ld) in classes:
+        p = coop_program(la, lb, lc, ld)
+        d = dict(cid=cid, la=la, lb=lb, lc=lc, ld=ld, S=p["S"], nacc=p["nacc"], nout=len(p["outs"]),
+                 vslots=p["vslots"], hslots=p["hslots"], vnode_off=len(vn), nvlev=len(p["vlev"]) - 1,
+                 vlev_off=len(vl), tgt_off=len(tg), hnode_off=len(hn), nhlev=len(p["hlev"]) - 1, hlev_off=len(hl),
+                 out_off=len(ou))
+        for (dst, s1, s2, s3, s4, s5, side, dr, k, ne, lvl) in p["vnodes"]:
+            assert max(dst, s1, s2, s3, s4, s5) < 65536
+            vn.append((dst | s1 << 16, s2 | s3 << 16, s4 | s5 << 16, side | dr << 1 | k << 3 | ne << 8))
+        vl += p["vlev"]
+        tg += p["targets"]
+        for (dst, s1, s2, side, dr, lvl) in p["hnodes"]:
+            assert max(dst, s1, s2) < 65536
+            hn.append((dst | s1 << 16, s2 | side << 16 | dr << 17))
+        hl += p["hlev"]
+        ou += p["outs"]
+        descs.append(d)
+    fields = ["cid", "la", "lb", "lc", "ld", "S", "nacc", "nout", "vslots", "hslots", "vnode_off", "nvlev", "vlev_off",
+              "tgt_off", "hnode_off", "nhlev", "hlev_off", "out_off"]
+    lines.append("struct CoopClass { int " + ", ".join(fields) + "; };")
+    lines.append(f"#define QX_NUM_COOP {len(descs)}")
+    lines.append("static const CoopClass g_coop_classes[QX_NUM_COOP] = {")
+    for d in descs:
+        lines.append("  {" + ", ".join(str(d[f]) for f in fields) + "},")
+    lines.append("};")
+    def arr(name, typ, vals, per):
+        out = [f"__device__ const {typ} {name}[{max(len(vals), 1)}] = {{"]
+        row = []
+        for v in vals:
+            row.append(per(v))
+            if len(row) == 8:
+                out.append("  " + ", ".join(row) + ",")
+                row = []
+        if row:
+            out.append("  " + ", ".join(row) + ",")
+        if not vals:
+            out.append("  {}" if typ.startswith("uint") else "  0")
+        out.append("};")
+        return out
+    lines += arr("g_coop_vnodes", "uint4", vn, lambda v: "{%du,%du,%du,%du}" % v)
+    lines += arr("g_coop_vlev", "int", vl, str)
+    lines += arr("g_coop_targets", "unsigned short", tg, str)
+    lines += arr("g_coop_hnodes", "uint2", hn, lambda v: "{%du,%du}" % v)
+    lines += arr("g_coop_hlev", "int", hl, str)
+    lines += arr("g_coop_outs", "unsigned short", ou, str)
+    return "\n".join(lines) + "\n"
+
+
 def pair_classes(lmax):
     return [(a, b) for a in range(lmax + 1) for b in range(a + 1)]
 
@@ -324,11 +541,22 @@ def main():
     hdr.append("#define QX_FOR_EACH_CLASS(X) " + " ".join(f"X({i}, {a}, {b}, {c}, {d})" for i, (a, b, c, d) in enumerate(qc)))
     hdr.append(f"#define QX_NUM_CLASSES {len(qc)}")
     hdr.append(f"#define QX_NUM_PAIR_CLASSES {len(pair_classes(lmax))}")
-    body = [gen_plain(*c) for c in qc]
+    hdr.append("#define QX_CLASS_NOUT " + "{" + ", ".join(str(ncart(a) * ncart(b) * ncart(c) * ncart(d)) for (a, b, c, d) in qc) + "}")
+    hdr.append("#define QX_CLASS_COOP " + "{" + ", ".join("1" if c in COOP_CLASSES else "0" for c in qc) + "}")
+    hdr.append("// X(class_id, LA, LB, LC, LD) for the classes with straight-line kernels")
+    hdr.append("#define QX_FOR_EACH_SL_CLASS(X) " + " ".join(f"X({i}, {a}, {b}, {c}, {d})" for i, (a, b, c, d) in enumerate(qc) if (a, b, c, d) not in COOP_CLASSES))
+    body = [gen_plain(*c) for c in qc if c not in COOP_CLASSES]
+    with open(os.path.join(here, "gen", "coop_tables.cuh"), "w") as f:
+        f.write(gen_coop([(i, c) for i, c in enumerate(qc) if c in COOP_CLASSES]))
     dbody = [gen_deriv(*c) for c in quartet_classes(lmax)]
     with open(os.path.join(here, "gen", "eri_classes.cuh"), "w") as f:
         f.write("\n".join(hdr) + "\n\n" + "\n\n".join(body) + "\n")
+    for fn in os.listdir(os.path.join(here, "gen")):
+        if fn.startswith("k_eri_") and fn.endswith(".cu"):
+            os.remove(os.path.join(here, "gen", fn))
     for i, (a, b, c, d) in enumerate(qc):
+        if (a, b, c, d) in COOP_CLASSES:
+            continue
         with open(os.path.join(here, "gen", f"k_eri_{i:02d}.cu"), "w") as f:
             f.write("// Generated by quax_b200/csrc/gen_eri.py -- do not edit by hand.\n")
             f.write(f"// ERI kernels of class ({a}{b}|{c}{d}).\n")

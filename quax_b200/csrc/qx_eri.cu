@@ -68,10 +68,26 @@ struct DeviceGuard {
     }
 };
 
-#define QX_ERI_ENTRY(id, a, b, c, d) &qx_launch_eri_##id,
-static const EriLaunch g_eri_launch[QX_NUM_CLASSES] = {QX_FOR_EACH_CLASS(QX_ERI_ENTRY)};
-#define QX_NOUT_ENTRY(id, a, b, c, d) EriCls<a, b, c, d>::NOUT,
-static const int g_class_nout[QX_NUM_CLASSES] = {QX_FOR_EACH_CLASS(QX_NOUT_ENTRY)};
+// Per-class launch table: straight-line kernels where generated, the
+// warp-cooperative engine for the large classes.
+static EriLaunch g_eri_launch[QX_NUM_CLASSES];
+static long long g_class_scratch[QX_NUM_CLASSES];
+static const int g_class_nout[QX_NUM_CLASSES] = QX_CLASS_NOUT;
+static const int g_class_coop[QX_NUM_CLASSES] = QX_CLASS_COOP;
+static int g_coop_idx[QX_NUM_CLASSES];
+static bool init_class_tables() {
+    for (int c = 0; c < QX_NUM_CLASSES; ++c) {
+        g_eri_launch[c] = nullptr;
+        g_class_scratch[c] = 0;
+        g_coop_idx[c] = g_class_coop[c] ? qx_coop_index(c) : -1;
+    }
+#define QX_SL_ENTRY(id, a, b, c, d)                            \
+    g_eri_launch[id] = &qx_launch_eri_##id;                    \
+    g_class_scratch[id] = qx::scratch_per_quartet<a, b, c, d>();
+    QX_FOR_EACH_SL_CLASS(QX_SL_ENTRY)
+    return true;
+}
+static const bool g_tables_ready = init_class_tables();
 
 // ------------------------------------------------------------------ Boys table --
 static void boys_table_host(std::vector<double>& tab) {
@@ -107,7 +123,24 @@ struct ClassWork {
     long long nq = 0;
     int2* d_q = nullptr;
     long long unique_base = 0;
+    long long prims = 0;       // primitive quartets of the class
+    int log2g = 0;             // lanes per quartet = 2^log2g
+    double* scratch = nullptr; // global accumulators (ACC_GLOBAL classes), owned
 };
+
+static constexpr int QX_NSTREAMS = 8;
+
+// Lanes per quartet: split a quartet's primitive loop over up to 32 lanes while
+// the class has too few quartets to fill the GPU and each lane keeps >= 8
+// primitive quartets of work.
+static int choose_log2g(long long nq, long long prims) {
+    int lg = 0;
+    const double avg = nq ? (double)prims / nq : 0.0;
+    while (lg < 5 && (nq << lg) < 150000 && avg / (1 << (lg + 1)) >= 8.0) ++lg;
+    return lg;
+}
+
+static long long launch_threads(long long nq, int log2g) { return (((nq << log2g) + 127) / 128) * 128; }
 
 struct qx_handle {
     int device = 0;
@@ -122,10 +155,16 @@ struct qx_handle {
     PairInfo* d_pairs = nullptr;
     double* d_boys = nullptr;
     int* d_err = nullptr;
+    double* d_scratch = nullptr;  // accumulators of classes too large for shared memory
+    long long scratch_len = 0;
     std::vector<double> K;  // nshell^2
     double kmax = 0.0;
     ClassWork work[QX_NUM_CLASSES];
     long long nunique = 0, unique_size = 0;
+    cudaStream_t streams[QX_NSTREAMS] = {};
+    cudaEvent_t done[QX_NSTREAMS] = {};
+    cudaEvent_t start = nullptr;
+    int order[QX_NUM_CLASSES];  // classes by decreasing primitive work
 };
 
 static int pair_index(int s1, int s2) { return s1 * (s1 + 1) / 2 + s2; }  // s1 >= s2
@@ -136,7 +175,13 @@ static void free_handle(qx_handle* h) {
     cudaFree(h->d_pairs);
     cudaFree(h->d_boys);
     cudaFree(h->d_err);
-    for (auto& w : h->work) cudaFree(w.d_q);
+    cudaFree(h->d_scratch);
+    for (auto& w : h->work) { cudaFree(w.d_q); cudaFree(w.scratch); }
+    for (int i = 0; i < QX_NSTREAMS; ++i) {
+        if (h->streams[i]) cudaStreamDestroy(h->streams[i]);
+        if (h->done[i]) cudaEventDestroy(h->done[i]);
+    }
+    if (h->start) cudaEventDestroy(h->start);
     delete h;
 }
 
@@ -147,7 +192,7 @@ static double dfact(int n) {
 }
 
 static int run_class(qx_handle* h, int cls, int mode, const int2* d_q, long long nq, double* out, long long n,
-                     long long base, cudaStream_t s) {
+                     long long base, cudaStream_t s, int log2g = 0, double* scratch = nullptr) {
     EriArgs a;
     a.quartets = d_q;
     a.nq = nq;
@@ -157,8 +202,11 @@ static int run_class(qx_handle* h, int cls, int mode, const int2* d_q, long long
     a.out = out;
     a.n = n;
     a.base = base;
+    a.scratch = scratch ? scratch : h->d_scratch;
+    a.log2g = g_class_coop[cls] ? 0 : log2g;
     a.err = h->d_err;
-    g_eri_launch[cls](a, mode, s);
+    if (g_class_coop[cls]) qx_launch_coop(g_coop_idx[cls], a, mode, s);
+    else g_eri_launch[cls](a, mode, s);
     QX_CUDA(cudaGetLastError());
     return QX_OK;
 }
@@ -286,6 +334,15 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
     cudaMemcpy(h->d_pairs, h->pairs.data(), sizeof(PairInfo) * np, cudaMemcpyHostToDevice);
     cudaMemcpy(h->d_boys, boys.data(), sizeof(double) * boys.size(), cudaMemcpyHostToDevice);
     cudaMemset(h->d_err, 0, sizeof(int));
+    // global accumulator scratch, sized for the largest launch that needs it
+    {
+        long long need = 0;
+        for (int c = 0; c < QX_NUM_CLASSES; ++c) need = std::max(need, g_class_scratch[c] * launch_threads(np, 0));
+        if (need) {
+            QX_ALLOC(h->d_scratch, sizeof(double) * need);
+            h->scratch_len = need;
+        }
+    }
     // Schwarz: diagonal quartets (P|P) of every pair
     {
         std::vector<std::vector<int2>> diag(QX_NUM_PAIR_CLASSES);
@@ -340,24 +397,49 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
     long long base = 0;
     for (int c = 0; c < QX_NUM_CLASSES; ++c) {
         auto& L = lists[c];
-        // counting sort by (bra nprim, ket nprim): equal trip counts within a warp
-        std::vector<long long> cnt(64 * 64 + 1, 0);
-        auto key = [&](const int2& q) { return (h->pairs[q.x].nprim - 1) * 64 + (h->pairs[q.y].nprim - 1); };
-        for (auto& q : L) cnt[std::min(key(q), 64 * 64 - 1) + 1]++;
-        for (int k = 0; k < 64 * 64; ++k) cnt[k + 1] += cnt[k];
+        // counting sort by (bra nprim, ket nprim), largest first: equal trip counts
+        // within a warp and the cheap quartets in the tail of the launch
+        const int NK = 64 * 64;
+        std::vector<long long> cnt(NK + 1, 0);
+        auto key = [&](const int2& q) {
+            return NK - 1 - std::min((h->pairs[q.x].nprim - 1) * 64 + (h->pairs[q.y].nprim - 1), NK - 1);
+        };
+        long long prims = 0;
+        for (auto& q : L) {
+            cnt[key(q) + 1]++;
+            prims += (long long)h->pairs[q.x].nprim * h->pairs[q.y].nprim;
+        }
+        for (int k = 0; k < NK; ++k) cnt[k + 1] += cnt[k];
         std::vector<int2> sorted(L.size());
-        for (auto& q : L) sorted[cnt[std::min(key(q), 64 * 64 - 1)]++] = q;
+        for (auto& q : L) sorted[cnt[key(q)]++] = q;
         ClassWork& w = h->work[c];
         w.nq = (long long)sorted.size();
+        w.prims = prims;
+        w.log2g = g_class_coop[c] ? 0 : choose_log2g(w.nq, prims);
         w.unique_base = base;
         base += w.nq * g_class_nout[c];
         h->nunique += w.nq;
         if (w.nq) {
             QX_ALLOC(w.d_q, sizeof(int2) * w.nq);
             cudaMemcpy(w.d_q, sorted.data(), sizeof(int2) * w.nq, cudaMemcpyHostToDevice);
+            if (g_class_scratch[c]) QX_ALLOC(w.scratch, sizeof(double) * g_class_scratch[c] * launch_threads(w.nq, w.log2g));
         }
     }
     h->unique_size = base;
+    for (int c = 0; c < QX_NUM_CLASSES; ++c) h->order[c] = c;
+    std::sort(h->order, h->order + QX_NUM_CLASSES,
+              [&](int x, int y) { return h->work[x].prims * g_class_nout[x] > h->work[y].prims * g_class_nout[y]; });
+    for (int i = 0; i < QX_NSTREAMS; ++i) {
+        if (cudaStreamCreateWithFlags(&h->streams[i], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&h->done[i], cudaEventDisableTiming) != cudaSuccess) {
+            free_handle(h);
+            return fail(QX_E_CUDA, "qx_initialize: stream creation failed");
+        }
+    }
+    if (cudaEventCreateWithFlags(&h->start, cudaEventDisableTiming) != cudaSuccess) {
+        free_handle(h);
+        return fail(QX_E_CUDA, "qx_initialize: event creation failed");
+    }
 #undef QX_ALLOC
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
@@ -399,16 +481,31 @@ static int check_err_word(qx_handle* h, cudaStream_t s) {
     return QX_OK;
 }
 
+// Launch every class on the handle's internal streams (largest work first,
+// round-robin), ordered after the caller's stream and joined back into it.
+static int run_all_classes(qx_handle* h, int mode, double* out, long long n, cudaStream_t s) {
+    QX_CUDA(cudaEventRecord(h->start, s));
+    for (int i = 0; i < QX_NSTREAMS; ++i) QX_CUDA(cudaStreamWaitEvent(h->streams[i], h->start, 0));
+    int k = 0;
+    for (int oi = 0; oi < QX_NUM_CLASSES; ++oi) {
+        const int c = h->order[oi];
+        const ClassWork& w = h->work[c];
+        if (!w.nq) continue;
+        cudaStream_t cs = h->streams[k++ % QX_NSTREAMS];
+        int rc = run_class(h, c, mode, w.d_q, w.nq, out, n, w.unique_base, cs, w.log2g, w.scratch);
+        if (rc) return rc;
+    }
+    for (int i = 0; i < QX_NSTREAMS; ++i) {
+        QX_CUDA(cudaEventRecord(h->done[i], h->streams[i]));
+        QX_CUDA(cudaStreamWaitEvent(s, h->done[i], 0));
+    }
+    return QX_OK;
+}
+
 static int eri_dense_dev(qx_handle* h, double* out, cudaStream_t s) {
     const long long n = h->nbf;
     QX_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * n * n * n * n, s));
-    for (int c = 0; c < QX_NUM_CLASSES; ++c) {
-        const ClassWork& w = h->work[c];
-        if (!w.nq) continue;
-        int rc = run_class(h, c, MODE_DENSE, w.d_q, w.nq, out, n, 0, s);
-        if (rc) return rc;
-    }
-    return QX_OK;
+    return run_all_classes(h, MODE_DENSE, out, n, s);
 }
 
 extern "C" int qx_compute_2e_int(qx_handle* h, double* out, int out_on_device, void* stream) {
@@ -437,12 +534,5 @@ extern "C" int qx_compute_2e_int(qx_handle* h, double* out, int out_on_device, v
 extern "C" int qx_eri_unique(qx_handle* h, double* out_dev, void* stream) {
     if (!h || !out_dev) return fail(QX_E_INVALID, "qx_eri_unique: NULL argument");
     DeviceGuard g(h->device);
-    cudaStream_t s = (cudaStream_t)stream;
-    for (int c = 0; c < QX_NUM_CLASSES; ++c) {
-        const ClassWork& w = h->work[c];
-        if (!w.nq) continue;
-        int rc = run_class(h, c, MODE_UNIQUE, w.d_q, w.nq, out_dev, 0, w.unique_base, s);
-        if (rc) return rc;
-    }
-    return QX_OK;
+    return run_all_classes(h, MODE_UNIQUE, out_dev, 0, (cudaStream_t)stream);
 }

@@ -20,80 +20,176 @@ struct EriArgs {
     double* out;
     long long n;     // MODE_DENSE: number of basis functions
     long long base;  // MODE_UNIQUE: offset of this class block
+    double* scratch; // ACC_GLOBAL classes: nq * group * NACC doubles
+    int log2g;       // log2 of the lanes cooperating on one quartet (0..5)
     int* err;
 };
 
-template <int LA, int LB, int LC, int LD, int MODE>
-__global__ void __launch_bounds__(128) k_eri(EriArgs a) {
-    using C = EriCls<LA, LB, LC, LD>;
-    const long long qi = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (qi >= a.nq) return;
-    const int2 pq = a.quartets[qi];
-    const PairInfo P = a.pairs[pq.x];
-    const PairInfo Q = a.pairs[pq.y];
-    double acc[C::NACC];
-#pragma unroll
-    for (int k = 0; k < C::NACC; ++k) acc[k] = 0.0;
-    for (int i = 0; i < P.nprim; ++i) {
-        const PrimPair p = a.prims[P.prim_off + i];
-        for (int j = 0; j < Q.nprim; ++j) {
-            const PrimPair r = a.prims[Q.prim_off + j];
-            PrimQ q;
-            double Fp[C::S + 1];
-            prim_setup<C::S>(p, r, a.boys, q, Fp);
-            C::vrr(acc, Fp, q);
+// Accumulator storage for the contracted [e0|f0] targets of one quartet.
+template <int N>
+struct RegAcc {
+    double v[N];
+    __device__ __forceinline__ double& operator()(int k) { return v[k]; }
+};
+struct StridedAcc {  // shared or global memory, element k of thread t at base[k*stride + t]
+    double* base;
+    long long stride;
+    __device__ __forceinline__ double& operator()(int k) { return base[(long long)k * stride]; }
+};
+
+// Accumulator placement per class: registers when small, shared memory (per
+// thread, conflict-free SoA) when mid-sized, global scratch when even 32 threads'
+// worth does not fit in shared memory.
+enum { ACC_REG = 0, ACC_SMEM = 1, ACC_GLOBAL = 2 };
+template <int NACC>
+struct AccPolicy {
+    static constexpr int kind = NACC <= 48 ? ACC_REG : (NACC <= 220 ? ACC_SMEM : ACC_GLOBAL);
+    static constexpr int bs = 128;
+    static constexpr int smem = kind == ACC_SMEM ? NACC * bs * 8 : 0;
+};
+
+template <int NA, int NB, int NC, int ND>
+struct UniqueStore {
+    double* out;
+    long long base, nq, qi;
+    __device__ __forceinline__ void operator()(int k, double v) { out[base + (long long)k * nq + qi] = v; }
+};
+
+template <int NA, int NB, int NC, int ND>
+struct SchwarzStore {
+    double mx = 0.0;
+    __device__ __forceinline__ void operator()(int k, double v) {
+        const int ab = k / (NC * ND), cd = k % (NC * ND);
+        if (ab == cd) mx = fmax(mx, fabs(v));
+    }
+};
+
+// Writes one element of a unique quartet to all its images in the dense n^4
+// tensor (8-fold permutational symmetry, images deduplicated by the flags).
+template <int NA, int NB, int NC, int ND>
+struct DenseStore {
+    double* __restrict__ out;
+    long long n;
+    int bf1, bf2, bf3, bf4;
+    bool s12, s34, sPQ;
+    __device__ __forceinline__ void operator()(int k, double v) {
+        const int id = k % ND, ic = (k / ND) % NC, ib = (k / (ND * NC)) % NB, ia = k / (ND * NC * NB);
+        const long long i = bf1 + ia, j = bf2 + ib, kk = bf3 + ic, l = bf4 + id;
+        out[((i * n + j) * n + kk) * n + l] = v;
+        if (s12) out[((j * n + i) * n + kk) * n + l] = v;
+        if (s34) out[((i * n + j) * n + l) * n + kk] = v;
+        if (s12 && s34) out[((j * n + i) * n + l) * n + kk] = v;
+        if (sPQ) {
+            out[((kk * n + l) * n + i) * n + j] = v;
+            if (s34) out[((l * n + kk) * n + i) * n + j] = v;
+            if (s12) out[((kk * n + l) * n + j) * n + i] = v;
+            if (s12 && s34) out[((l * n + kk) * n + j) * n + i] = v;
         }
     }
-    double o[C::NOUT];
-    C::hrr(acc, o, P.ABx, P.ABy, P.ABz, Q.ABx, Q.ABy, Q.ABz);
-    constexpr int NA = ncart_h(LA), NB = ncart_h(LB), NC = ncart_h(LC), ND = ncart_h(LD);
-    if constexpr (MODE == MODE_UNIQUE) {
+};
+
+// Primitive loop of one contracted quartet.  The G = 2^log2g lanes of a group
+// take primitive quartets t = sub, sub+G, ...; afterwards the group's partial
+// accumulators are summed with butterfly shuffles into lane sub == 0.
+template <class C, class Acc>
+__device__ __forceinline__ void contract_quartet(const EriArgs& a, const PairInfo& P, const PairInfo& Q, Acc& acc,
+                                                 int sub, bool active) {
 #pragma unroll
-        for (int k = 0; k < C::NOUT; ++k) a.out[a.base + (long long)k * a.nq + qi] = o[k];
-    } else if constexpr (MODE == MODE_SCHWARZ) {
-        double mx = 0.0;
-#pragma unroll
-        for (int ia = 0; ia < NA; ++ia)
-#pragma unroll
-            for (int ib = 0; ib < NB; ++ib) mx = fmax(mx, fabs(o[((ia * NB + ib) * NC + ia) * ND + ib]));
-        a.out[pq.x] = mx;
-    } else {
-        const long long n = a.n;
-        const bool s12 = P.s1 != P.s2, s34 = Q.s1 != Q.s2, sPQ = pq.x != pq.y;
-        double* __restrict__ out = a.out;
-#pragma unroll
-        for (int ia = 0; ia < NA; ++ia)
-#pragma unroll
-            for (int ib = 0; ib < NB; ++ib)
-#pragma unroll
-                for (int ic = 0; ic < NC; ++ic)
-#pragma unroll
-                    for (int id = 0; id < ND; ++id) {
-                        const double v = o[((ia * NB + ib) * NC + ic) * ND + id];
-                        const long long i = P.bf1 + ia, j = P.bf2 + ib, k = Q.bf1 + ic, l = Q.bf2 + id;
-                        out[((i * n + j) * n + k) * n + l] = v;
-                        if (s12) out[((j * n + i) * n + k) * n + l] = v;
-                        if (s34) out[((i * n + j) * n + l) * n + k] = v;
-                        if (s12 && s34) out[((j * n + i) * n + l) * n + k] = v;
-                        if (sPQ) {
-                            out[((k * n + l) * n + i) * n + j] = v;
-                            if (s34) out[((l * n + k) * n + i) * n + j] = v;
-                            if (s12) out[((k * n + l) * n + j) * n + i] = v;
-                            if (s12 && s34) out[((l * n + k) * n + j) * n + i] = v;
-                        }
-                    }
+    for (int k = 0; k < C::NACC; ++k) acc(k) = 0.0;
+    const int nk = Q.nprim;
+    const int ntot = active ? P.nprim * nk : 0;
+    const int G = 1 << a.log2g;
+    for (int t = sub; t < ntot; t += G) {
+        const int i = t / nk, j = t - i * nk;
+        const PrimPair p = a.prims[P.prim_off + i];
+        const PrimPair r = a.prims[Q.prim_off + j];
+        PrimQ q;
+        double Fp[C::S + 1];
+        prim_setup<C::S>(p, r, a.boys, q, Fp);
+        C::vrr(acc, Fp, q);
+    }
+    if (a.log2g) {
+#pragma unroll 1
+        for (int k = 0; k < C::NACC; ++k) {
+            double v = acc(k);
+            for (int off = G >> 1; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+            acc(k) = v;
+        }
     }
 }
 
+template <class C, int LA, int LB, int LC, int LD, int MODE, class Acc>
+__device__ __noinline__ void finish_quartet(const EriArgs& a, const PairInfo& P, const PairInfo& Q, int2 pq,
+                                            long long qi, Acc acc) {
+    constexpr int NA = ncart_h(LA), NB = ncart_h(LB), NC = ncart_h(LC), ND = ncart_h(LD);
+    if constexpr (MODE == MODE_UNIQUE) {
+        UniqueStore<NA, NB, NC, ND> st{a.out, a.base, a.nq, qi};
+        C::hrr(acc, st, P.ABx, P.ABy, P.ABz, Q.ABx, Q.ABy, Q.ABz);
+    } else if constexpr (MODE == MODE_SCHWARZ) {
+        SchwarzStore<NA, NB, NC, ND> st;
+        C::hrr(acc, st, P.ABx, P.ABy, P.ABz, Q.ABx, Q.ABy, Q.ABz);
+        a.out[pq.x] = st.mx;
+    } else {
+        DenseStore<NA, NB, NC, ND> st{a.out, a.n, P.bf1, P.bf2, Q.bf1, Q.bf2, P.s1 != P.s2, Q.s1 != Q.s2, pq.x != pq.y};
+        C::hrr(acc, st, P.ABx, P.ABy, P.ABz, Q.ABx, Q.ABy, Q.ABz);
+    }
+}
+
+template <int LA, int LB, int LC, int LD, int MODE>
+__global__ void __launch_bounds__(AccPolicy<EriCls<LA, LB, LC, LD>::NACC>::bs) k_eri(EriArgs a) {
+    using C = EriCls<LA, LB, LC, LD>;
+    using Pol = AccPolicy<C::NACC>;
+    const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long qi = gt >> a.log2g;
+    const int sub = (int)(gt & ((1 << a.log2g) - 1));
+    const bool active = qi < a.nq;
+    // every lane stays to the end: the group reduction shuffles over the full warp
+    const int2 pq = active ? a.quartets[qi] : make_int2(0, 0);
+    const PairInfo P = a.pairs[pq.x];
+    const PairInfo Q = a.pairs[pq.y];
+    if constexpr (Pol::kind == ACC_REG) {
+        RegAcc<C::NACC> acc;
+        contract_quartet<C>(a, P, Q, acc, sub, active);
+        if (active && sub == 0) finish_quartet<C, LA, LB, LC, LD, MODE>(a, P, Q, pq, qi, acc);
+    } else if constexpr (Pol::kind == ACC_SMEM) {
+        extern __shared__ double smem_acc[];
+        StridedAcc acc{smem_acc + threadIdx.x, Pol::bs};
+        contract_quartet<C>(a, P, Q, acc, sub, active);
+        if (active && sub == 0) finish_quartet<C, LA, LB, LC, LD, MODE>(a, P, Q, pq, qi, acc);
+    } else {
+        const long long nthreads = (long long)gridDim.x * blockDim.x;
+        StridedAcc acc{a.scratch + gt, nthreads};
+        contract_quartet<C>(a, P, Q, acc, sub, active);
+        if (active && sub == 0) finish_quartet<C, LA, LB, LC, LD, MODE>(a, P, Q, pq, qi, acc);
+    }
+}
 
 template <int LA, int LB, int LC, int LD>
 void launch_eri(const EriArgs& a, int mode, cudaStream_t s) {
-    const int bs = 128;
-    const long long nb = (a.nq + bs - 1) / bs;
+    using Pol = AccPolicy<EriCls<LA, LB, LC, LD>::NACC>;
+    const int bs = Pol::bs;
+    const long long nb = ((a.nq << a.log2g) + bs - 1) / bs;
     if (nb == 0) return;
-    if (mode == MODE_DENSE) k_eri<LA, LB, LC, LD, MODE_DENSE><<<(unsigned)nb, bs, 0, s>>>(a);
-    else if (mode == MODE_UNIQUE) k_eri<LA, LB, LC, LD, MODE_UNIQUE><<<(unsigned)nb, bs, 0, s>>>(a);
-    else if constexpr (LA == LC && LB == LD) k_eri<LA, LB, LC, LD, MODE_SCHWARZ><<<(unsigned)nb, bs, 0, s>>>(a);
+    if (mode == MODE_DENSE) {
+        auto k = k_eri<LA, LB, LC, LD, MODE_DENSE>;
+        if (Pol::smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, Pol::smem);
+        k<<<(unsigned)nb, bs, Pol::smem, s>>>(a);
+    } else if (mode == MODE_UNIQUE) {
+        auto k = k_eri<LA, LB, LC, LD, MODE_UNIQUE>;
+        if (Pol::smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, Pol::smem);
+        k<<<(unsigned)nb, bs, Pol::smem, s>>>(a);
+    } else if constexpr (LA == LC && LB == LD) {
+        auto k = k_eri<LA, LB, LC, LD, MODE_SCHWARZ>;
+        if (Pol::smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, Pol::smem);
+        k<<<(unsigned)nb, bs, Pol::smem, s>>>(a);
+    }
+}
+
+// Doubles of global scratch a class needs per quartet (0 unless ACC_GLOBAL).
+template <int LA, int LB, int LC, int LD>
+constexpr long long scratch_per_quartet() {
+    using C = EriCls<LA, LB, LC, LD>;
+    return AccPolicy<C::NACC>::kind == ACC_GLOBAL ? C::NACC : 0;
 }
 
 typedef void (*EriLaunch)(const EriArgs&, int mode, cudaStream_t);
@@ -102,8 +198,11 @@ typedef void (*EriLaunch)(const EriArgs&, int mode, cudaStream_t);
 
 // one launcher per class, defined in gen/k_eri_<id>.cu
 #define QX_DECLARE_LAUNCH(id, a, b, c, d) void qx_launch_eri_##id(const qx::EriArgs&, int, cudaStream_t);
-QX_FOR_EACH_CLASS(QX_DECLARE_LAUNCH)
+QX_FOR_EACH_SL_CLASS(QX_DECLARE_LAUNCH)
+int qx_coop_index(int cls);
+void qx_launch_coop(int coop_idx, const qx::EriArgs& a, int mode, cudaStream_t s);
 #define QX_DEFINE_LAUNCH(id, a, b, c, d) \
     void qx_launch_eri_##id(const qx::EriArgs& x, int m, cudaStream_t s) { qx::launch_eri<a, b, c, d>(x, m, s); }
+#define QX_SCRATCH_ENTRY(id, a, b, c, d) qx::scratch_per_quartet<a, b, c, d>(),
 
 
