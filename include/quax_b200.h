@@ -91,11 +91,34 @@ int qx_schwarz(qx_handle *h, double *K, double *kmax);
  * screened-out quartets are zero. */
 int qx_compute_2e_int(qx_handle *h, double *out, int out_on_device, void *stream);
 
-/* Every screened unique quartet's contracted Cartesian block, written
- * class by class (canonical shell order within a quartet: higher AM first).  The
- * order is documented by qx_unique_layout.  No counterpart in the reference (it only
- * produces the dense tensor); this is the throughput path. Device memory only. */
+/* Every screened unique quartet's contracted Cartesian block, written class by
+ * class (canonical shell order within a quartet: higher AM first), element-major
+ * within a class.  No counterpart in the reference (it only produces the dense
+ * tensor); this is the throughput path.  Device memory only. */
 int qx_eri_unique(qx_handle *h, double *out_dev, void *stream);
+
+/* Replaces eri_deriv_core(order) (libint_interface.cc:2582-2779): the full
+ * first-derivative tensor, 3*natom*n^4 doubles in the layout (3N, n, n, n, n),
+ * nuclear index 3*atom + xyz.  Quartets whose four shells sit on one atom are
+ * skipped (zero), as in the reference.  order must be 1 in this build. */
+int qx_eri_deriv_core(qx_handle *h, int order, double *out, int out_on_device, void *stream);
+
+/* Replaces compute_2e_deriv("eri", 0., deriv_vec) (libint_interface.cc:1097-1335):
+ * one n^4 derivative slice selected by deriv_vec[3*natom] (non-negative counts;
+ * total order must be 1 in this build). */
+int qx_compute_2e_deriv(qx_handle *h, const int *deriv_vec, int len, double *out, int out_on_device,
+                        void *stream);
+
+/* Adjoint (contracted) gradient, no counterpart in the reference, which obtains it
+ * by jacfwd through the 3N x n^4 tensor (quax/methods/hartree_fock.py:79-80 with
+ * quax/integrals/tei.py:336-340):
+ *     grad[3*atom + xyz] = sum_ijkl Gamma_ijkl d(ij|kl)/dR_{atom,xyz},
+ *     Gamma_ijkl = cj * D_ij D_kl + ck * D_ik D_jl   (D symmetric, n x n, row-major).
+ * For the RHF energy of the reference (E_2e = 2 sum Gamma G with cj = 1,
+ * ck = -1/2) pass cj = 2, ck = -1.  grad (3*natom doubles) is overwritten.  D and
+ * grad are device pointers when on_device = 1, host pointers otherwise. */
+int qx_grad_adjoint(qx_handle *h, const double *D, double cj, double ck, double *grad, int on_device,
+                    void *stream);
 
 #ifdef __cplusplus
 }

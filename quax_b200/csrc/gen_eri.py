@@ -511,6 +511,155 @@ def gen_coop(classes):
     return "\n".join(lines) + "\n"
 
 
+# ----------------------------------------------------------------------------------
+# First-derivative programs (cooperative engine).  Accumulator sets, in order:
+#   U  = sum [e0|f0]          e in [la-1, lab],   f in [lc-1, lcd]
+#   WA = sum 2 alpha [e0|f0]  e in [la+1, lab+1], f in [lc, lcd]
+#   WB = sum 2 beta  [e0|f0]  e in [la, lab+1],   f in [lc, lcd]
+#   WC = sum 2 gamma [e0|f0]  e in [la, lab],     f in [lc+1, lcd+1]
+# HRR outputs: 9 blocks (A_x,A_y,A_z,B_x,..,C_z) of n1*n2*n3*n4 each:
+#   dA_i = (a+1_i b|cd)_WA - a_i (a-1_i b|cd)_U   (likewise B on b, C on c);
+# combination nodes use g = -k (geometry slots 6.. hold -1, -2, -3, -4).
+# ----------------------------------------------------------------------------------
+class HRRMulti:
+    def __init__(self, spaces):
+        self.spaces = spaces  # name -> (AccSpace, offset)
+        self.slot = {}
+        self.nodes = []
+        self.level = {}
+        self.next = sum(sp.size for sp, _ in spaces.values())
+
+    def _new(self, s1, s2, side, dr):
+        lvl = 1 + max(self.level.get(s1, 0), self.level.get(s2, 0))
+        dst = self.next
+        self.next += 1
+        self.nodes.append((dst, s1, s2, side, dr, lvl))
+        self.level[dst] = lvl
+        return dst
+
+    def get(self, sp, a, b, c, d):
+        key = (sp, a, b, c, d)
+        if key in self.slot:
+            return self.slot[key]
+        if sum(d) > 0:
+            j = first_dir(d)
+            dst = self._new(self.get(sp, a, b, sh(c, j, 1), sh(d, j, -1)), self.get(sp, a, b, c, sh(d, j, -1)), 1, j)
+        elif sum(b) > 0:
+            i = first_dir(b)
+            dst = self._new(self.get(sp, sh(a, i, 1), sh(b, i, -1), c, d), self.get(sp, a, sh(b, i, -1), c, d), 0, i)
+        else:
+            acc, off = self.spaces[sp]
+            dst = off + acc.index(a, c)
+        self.slot[key] = dst
+        return dst
+
+    def combine(self, x, y, k):
+        """x - k*y (k = 1..4)"""
+        return self._new(x, y, 2, k - 1)
+
+
+def coop_deriv_program(la, lb, lc, ld):
+    lab, lcd = la + lb, lc + ld
+    S = lab + lcd + 1
+    spaces = [("U", AccSpace("U", la - 1, lab, lc - 1, lcd)), ("WA", AccSpace("WA", la + 1, lab + 1, lc, lcd)),
+              ("WB", AccSpace("WB", la, lab + 1, lc, lcd)), ("WC", AccSpace("WC", la, lab, lc + 1, lcd + 1))]
+    vd = VRRDag(S)
+    targets = []
+    sizes = []
+    for name, sp in spaces:
+        sizes.append(sp.size)
+        targets += [vd.get(e, f, 0) for e, f in sp.targets()]
+    vnodes = sorted(vd.nodes, key=lambda n: n[-1])
+    vlev = [sum(1 for n in vnodes if n[-1] < lv) for lv in range(1, max(n[-1] for n in vnodes) + 1)] + [len(vnodes)]
+    offs = {}
+    o = 0
+    for name, sp in spaces:
+        offs[name] = (sp, o)
+        o += sp.size
+    hm = HRRMulti(offs)
+    outs = [None] * (9 * ncart(la) * ncart(lb) * ncart(lc) * ncart(ld))
+    nout = ncart(la) * ncart(lb) * ncart(lc) * ncart(ld)
+    k = 0
+    for a in comps(la):
+        for b in comps(lb):
+            for c in comps(lc):
+                for d in comps(ld):
+                    for i in range(3):
+                        x = hm.get("WA", sh(a, i, 1), b, c, d)
+                        outs[(0 + i) * nout + k] = hm.combine(x, hm.get("U", sh(a, i, -1), b, c, d), a[i]) if a[i] else x
+                        x = hm.get("WB", a, sh(b, i, 1), c, d)
+                        outs[(3 + i) * nout + k] = hm.combine(x, hm.get("U", a, sh(b, i, -1), c, d), b[i]) if b[i] else x
+                        x = hm.get("WC", a, b, sh(c, i, 1), d)
+                        outs[(6 + i) * nout + k] = hm.combine(x, hm.get("U", a, b, sh(c, i, -1), d), c[i]) if c[i] else x
+                    k += 1
+    nacc = sum(sizes)
+    # every output must be its own HRR node: the epilogue runs inline when the
+    # node is evaluated, so outputs are not kept to the end
+    # (an output that is a leaf, or a node another output already owns, gets an
+    # identity node V[sl] + 0 * V[sl])
+    owner = {}
+    for ob, sl in enumerate(outs):
+        if sl < nacc or sl in owner:
+            sl = hm._new(sl, sl, 3, 0)
+            outs[ob] = sl
+        owner[sl] = ob
+    hnodes = sorted(hm.nodes, key=lambda n: n[-1])
+    hout = [owner.get(n[0], 0xFFFF) for n in hnodes]
+    hlev = [sum(1 for n in hnodes if n[-1] < lv) for lv in range(1, max(n[-1] for n in hnodes) + 1)]
+    hlev.append(len(hnodes))
+    vnodes, targets, vslots = _realloc([(n[0], n[1:6], n[-1]) for n in vnodes], vnodes, targets, S + 2, "v")
+    hnodes, _, hslots = _realloc([(n[0], n[1:3], n[-1]) for n in hnodes], hnodes, [], nacc, "h")
+    return dict(S=S, vnodes=vnodes, vlev=vlev, targets=targets, hnodes=hnodes, hlev=hlev, hout=hout, vslots=vslots,
+                hslots=hslots, nacc=nacc, sizes=sizes, nout=nout)
+
+
+def gen_coop_deriv(classes):
+    lines = ["// Generated by quax_b200/csrc/gen_eri.py -- do not edit by hand.",
+             "// First-derivative programs of the cooperative engine.", "#pragma once", "#include <stdint.h>", ""]
+    vn, vl, tg, hn, hl, ou = [], [], [], [], [], []
+    descs = []
+    for cid, (la, lb, lc, ld) in classes:
+        p = coop_deriv_program(la, lb, lc, ld)
+        assert len(p["hout"]) == len(p["hnodes"])
+        d = dict(cid=cid, la=la, lb=lb, lc=lc, ld=ld, S=p["S"], nacc=p["nacc"], nu=p["sizes"][0], na=p["sizes"][1],
+                 nb=p["sizes"][2], nc=p["sizes"][3], nout=p["nout"], vslots=p["vslots"], hslots=p["hslots"],
+                 vnode_off=len(vn), nvlev=len(p["vlev"]) - 1, vlev_off=len(vl), tgt_off=len(tg), hnode_off=len(hn),
+                 nhlev=len(p["hlev"]) - 1, hlev_off=len(hl), out_off=len(ou))
+        for (dst, s1, s2, s3, s4, s5, side, dr, k, ne, lvl) in p["vnodes"]:
+            assert max(dst, s1, s2, s3, s4, s5) < 65536
+            vn.append((dst | s1 << 16, s2 | s3 << 16, s4 | s5 << 16, side | dr << 1 | k << 3 | ne << 8))
+        vl += p["vlev"]
+        tg += p["targets"]
+        for (dst, s1, s2, side, dr, lvl) in p["hnodes"]:
+            assert max(dst, s1, s2) < 65536
+            hn.append((dst | s1 << 16, s2 | side << 16 | dr << 18))
+        hl += p["hlev"]
+        ou += p["hout"]
+        descs.append(d)
+    fields = ["cid", "la", "lb", "lc", "ld", "S", "nacc", "nu", "na", "nb", "nc", "nout", "vslots", "hslots",
+              "vnode_off", "nvlev", "vlev_off", "tgt_off", "hnode_off", "nhlev", "hlev_off", "out_off"]
+    lines.append("struct DerClass { int " + ", ".join(fields) + "; };")
+    lines.append(f"#define QX_NUM_DER {len(descs)}")
+    lines.append("static const DerClass g_der_classes[QX_NUM_DER] = {")
+    for d in descs:
+        lines.append("  {" + ", ".join(str(d[f]) for f in fields) + "},")
+    lines.append("};")
+
+    def arr(name, typ, vals, per):
+        out = [f"__device__ const {typ} {name}[{max(len(vals), 1)}] = {{"]
+        for i0 in range(0, len(vals), 8):
+            out.append("  " + ", ".join(per(v) for v in vals[i0:i0 + 8]) + ",")
+        out.append("};")
+        return out
+    lines += arr("g_der_vnodes", "uint4", vn, lambda v: "{%du,%du,%du,%du}" % v)
+    lines += arr("g_der_vlev", "int", vl, str)
+    lines += arr("g_der_targets", "unsigned short", tg, str)
+    lines += arr("g_der_hnodes", "uint2", hn, lambda v: "{%du,%du}" % v)
+    lines += arr("g_der_hlev", "int", hl, str)
+    lines += arr("g_der_outs", "unsigned short", ou, str)
+    return "\n".join(lines) + "\n"
+
+
 def pair_classes(lmax):
     return [(a, b) for a in range(lmax + 1) for b in range(a + 1)]
 
@@ -548,7 +697,6 @@ def main():
     body = [gen_plain(*c) for c in qc if c not in COOP_CLASSES]
     with open(os.path.join(here, "gen", "coop_tables.cuh"), "w") as f:
         f.write(gen_coop([(i, c) for i, c in enumerate(qc) if c in COOP_CLASSES]))
-    dbody = [gen_deriv(*c) for c in quartet_classes(lmax)]
     with open(os.path.join(here, "gen", "eri_classes.cuh"), "w") as f:
         f.write("\n".join(hdr) + "\n\n" + "\n\n".join(body) + "\n")
     for fn in os.listdir(os.path.join(here, "gen")):
@@ -562,8 +710,8 @@ def main():
             f.write(f"// ERI kernels of class ({a}{b}|{c}{d}).\n")
             f.write('#include "../qx_kernels.cuh"\n')
             f.write(f"QX_DEFINE_LAUNCH({i}, {a}, {b}, {c}, {d})\n")
-    with open(os.path.join(here, "gen", "der_classes.cuh"), "w") as f:
-        f.write("\n".join(hdr[:3] + ["#include \"eri_classes.cuh\""]) + "\n\n" + "\n\n".join(dbody) + "\n")
+    with open(os.path.join(here, "gen", "der_tables.cuh"), "w") as f:
+        f.write(gen_coop_deriv(list(enumerate(qc))))
 
 
 if __name__ == "__main__":

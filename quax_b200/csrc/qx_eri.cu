@@ -75,11 +75,18 @@ static long long g_class_scratch[QX_NUM_CLASSES];
 static const int g_class_nout[QX_NUM_CLASSES] = QX_CLASS_NOUT;
 static const int g_class_coop[QX_NUM_CLASSES] = QX_CLASS_COOP;
 static int g_coop_idx[QX_NUM_CLASSES];
+static int g_der_idx[QX_NUM_CLASSES];
+
+int qx_der_index(int cls);
+void qx_launch_der(int der_idx, const qx::EriArgs& a, int mode, const double* D, double cj, double ck, double* grad,
+                   int slice, cudaStream_t s);
+enum { QX_MODE_DER_DENSE = 10, QX_MODE_DER_SLICE = 11, QX_MODE_GRAD = 12 };
 static bool init_class_tables() {
     for (int c = 0; c < QX_NUM_CLASSES; ++c) {
         g_eri_launch[c] = nullptr;
         g_class_scratch[c] = 0;
         g_coop_idx[c] = g_class_coop[c] ? qx_coop_index(c) : -1;
+        g_der_idx[c] = qx_der_index(c);
     }
 #define QX_SL_ENTRY(id, a, b, c, d)                            \
     g_eri_launch[id] = &qx_launch_eri_##id;                    \
@@ -535,4 +542,134 @@ extern "C" int qx_eri_unique(qx_handle* h, double* out_dev, void* stream) {
     if (!h || !out_dev) return fail(QX_E_INVALID, "qx_eri_unique: NULL argument");
     DeviceGuard g(h->device);
     return run_all_classes(h, MODE_UNIQUE, out_dev, 0, (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------- derivatives --
+static EriArgs class_args(qx_handle* h, int c, double* out) {
+    const ClassWork& w = h->work[c];
+    EriArgs a;
+    a.quartets = w.d_q;
+    a.nq = w.nq;
+    a.pairs = h->d_pairs;
+    a.prims = h->d_prims;
+    a.boys = h->d_boys;
+    a.out = out;
+    a.n = h->nbf;
+    a.base = 0;
+    a.scratch = nullptr;
+    a.log2g = 0;
+    a.err = h->d_err;
+    return a;
+}
+
+// Every class through the derivative engine on the internal streams, joined
+// back into `s`.
+static int run_all_deriv(qx_handle* h, int mode, double* out, const double* D, double cj, double ck, double* grad,
+                         int slice, cudaStream_t s) {
+    QX_CUDA(cudaEventRecord(h->start, s));
+    for (int i = 0; i < QX_NSTREAMS; ++i) QX_CUDA(cudaStreamWaitEvent(h->streams[i], h->start, 0));
+    int k = 0;
+    for (int oi = 0; oi < QX_NUM_CLASSES; ++oi) {
+        const int c = h->order[oi];
+        if (!h->work[c].nq) continue;
+        if (g_der_idx[c] < 0) return fail(QX_E_UNSUPPORTED, "no derivative program for class %d", c);
+        qx_launch_der(g_der_idx[c], class_args(h, c, out), mode, D, cj, ck, grad, slice, h->streams[k++ % QX_NSTREAMS]);
+        QX_CUDA(cudaGetLastError());
+    }
+    for (int i = 0; i < QX_NSTREAMS; ++i) {
+        QX_CUDA(cudaEventRecord(h->done[i], h->streams[i]));
+        QX_CUDA(cudaStreamWaitEvent(s, h->done[i], 0));
+    }
+    return QX_OK;
+}
+
+// Stages a host output buffer through the device when out_on_device == 0.
+template <class F>
+static int with_output(qx_handle* h, double* out, size_t count, int out_on_device, cudaStream_t s, F&& body) {
+    if (out_on_device) return body(out);
+    double* d = nullptr;
+    if (cudaMalloc((void**)&d, sizeof(double) * count) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(QX_E_NOMEM, "cannot stage %zu bytes on the device", sizeof(double) * count);
+    }
+    int rc = body(d);
+    if (!rc) {
+        cudaError_t e = cudaMemcpyAsync(out, d, sizeof(double) * count, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) rc = fail(QX_E_CUDA, "copy-out failed: %s", cudaGetErrorString(e));
+    }
+    cudaFree(d);
+    if (!rc) rc = check_err_word(h, s);
+    return rc;
+}
+
+extern "C" int qx_eri_deriv_core(qx_handle* h, int order, double* out, int out_on_device, void* stream) {
+    if (!h || !out) return fail(QX_E_INVALID, "qx_eri_deriv_core: NULL argument");
+    if (order != 1) return fail(QX_E_UNSUPPORTED, "qx_eri_deriv_core: derivative order %d (this build: 1)", order);
+    DeviceGuard g(h->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const long long n = h->nbf, n4 = n * n * n * n;
+    const size_t count = (size_t)(3 * h->natom) * (size_t)n4;
+    return with_output(h, out, count, out_on_device, s, [&](double* d) {
+        QX_CUDA(cudaMemsetAsync(d, 0, sizeof(double) * count, s));
+        return run_all_deriv(h, QX_MODE_DER_DENSE, d, nullptr, 0.0, 0.0, nullptr, -1, s);
+    });
+}
+
+extern "C" int qx_compute_2e_deriv(qx_handle* h, const int* deriv_vec, int len, double* out, int out_on_device,
+                                   void* stream) {
+    if (!h || !out || !deriv_vec) return fail(QX_E_INVALID, "qx_compute_2e_deriv: NULL argument");
+    if (len != 3 * h->natom)
+        return fail(QX_E_INVALID, "qx_compute_2e_deriv: deriv_vec has %d entries, expected 3*natom = %d", len,
+                    3 * h->natom);
+    int order = 0, idx = -1;
+    for (int i = 0; i < len; ++i) {
+        if (deriv_vec[i] < 0) return fail(QX_E_INVALID, "qx_compute_2e_deriv: negative entry in deriv_vec");
+        order += deriv_vec[i];
+        if (deriv_vec[i]) idx = i;
+    }
+    if (order != 1)
+        return fail(QX_E_UNSUPPORTED, "qx_compute_2e_deriv: derivative order %d (this build: 1)", order);
+    DeviceGuard g(h->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const long long n = h->nbf, n4 = n * n * n * n;
+    return with_output(h, out, (size_t)n4, out_on_device, s, [&](double* d) {
+        QX_CUDA(cudaMemsetAsync(d, 0, sizeof(double) * n4, s));
+        return run_all_deriv(h, QX_MODE_DER_SLICE, d, nullptr, 0.0, 0.0, nullptr, idx, s);
+    });
+}
+
+extern "C" int qx_grad_adjoint(qx_handle* h, const double* D, double cj, double ck, double* grad, int on_device,
+                               void* stream) {
+    if (!h || !D || !grad) return fail(QX_E_INVALID, "qx_grad_adjoint: NULL argument");
+    if (!std::isfinite(cj) || !std::isfinite(ck)) return fail(QX_E_INVALID, "qx_grad_adjoint: non-finite coefficient");
+    DeviceGuard g(h->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const long long n = h->nbf;
+    const int N3 = 3 * h->natom;
+    if (on_device) {
+        QX_CUDA(cudaMemsetAsync(grad, 0, sizeof(double) * N3, s));
+        return run_all_deriv(h, QX_MODE_GRAD, nullptr, D, cj, ck, grad, -1, s);
+    }
+    double *dD = nullptr, *dg = nullptr;
+    if (cudaMalloc((void**)&dD, sizeof(double) * n * n) != cudaSuccess ||
+        cudaMalloc((void**)&dg, sizeof(double) * N3) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(dD);
+        return fail(QX_E_NOMEM, "qx_grad_adjoint: staging allocation failed");
+    }
+    int rc = QX_OK;
+    cudaError_t e = cudaMemcpyAsync(dD, D, sizeof(double) * n * n, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dg, 0, sizeof(double) * N3, s);
+    if (e != cudaSuccess) rc = fail(QX_E_CUDA, "qx_grad_adjoint: %s", cudaGetErrorString(e));
+    if (!rc) rc = run_all_deriv(h, QX_MODE_GRAD, nullptr, dD, cj, ck, dg, -1, s);
+    if (!rc) {
+        e = cudaMemcpyAsync(grad, dg, sizeof(double) * N3, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) rc = fail(QX_E_CUDA, "qx_grad_adjoint: %s", cudaGetErrorString(e));
+    }
+    cudaFree(dD);
+    cudaFree(dg);
+    if (!rc) rc = check_err_word(h, s);
+    return rc;
 }

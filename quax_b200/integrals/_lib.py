@@ -42,6 +42,9 @@ SIGNATURES = {
     "qx_schwarz": (C.c_int, [_vp, _dp, _dp]),
     "qx_compute_2e_int": (C.c_int, [_vp, _vp, C.c_int, _vp]),
     "qx_eri_unique": (C.c_int, [_vp, _vp, _vp]),
+    "qx_eri_deriv_core": (C.c_int, [_vp, C.c_int, _vp, C.c_int, _vp]),
+    "qx_compute_2e_deriv": (C.c_int, [_vp, _ip, C.c_int, _vp, C.c_int, _vp]),
+    "qx_grad_adjoint": (C.c_int, [_vp, _vp, C.c_double, C.c_double, _vp, C.c_int, _vp]),
 }
 
 _LIB = None

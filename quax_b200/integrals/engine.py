@@ -115,3 +115,46 @@ class EriEngine:
                 "qx_eri_unique",
             )
         return out
+
+    # -- derivatives ----------------------------------------------------------
+    def eri_deriv_core(self, order: int = 1, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+        """Dense (3N, n, n, n, n) first-derivative tensor on the device (reference layout)."""
+        n = self.nbf
+        shape = (3 * self.natom, n, n, n, n)
+        if out is None:
+            out = torch.empty(shape, dtype=torch.float64, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.check(
+                _lib.load().qx_eri_deriv_core(self.handle, int(order), C.c_void_p(out.data_ptr()), 1,
+                                              C.c_void_p(_stream_ptr(stream))),
+                "qx_eri_deriv_core",
+            )
+        return out
+
+    def eri_deriv(self, deriv_vec, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+        """One (n,n,n,n) derivative slice for an integer deriv_vec of length 3N."""
+        dv = np.ascontiguousarray(np.asarray(deriv_vec, dtype=np.int32).reshape(-1))
+        n = self.nbf
+        if out is None:
+            out = torch.empty((n, n, n, n), dtype=torch.float64, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.check(
+                _lib.load().qx_compute_2e_deriv(self.handle, _lib.iptr(dv), dv.size, C.c_void_p(out.data_ptr()), 1,
+                                                C.c_void_p(_stream_ptr(stream))),
+                "qx_compute_2e_deriv",
+            )
+        return out
+
+    def grad_adjoint(self, D: torch.Tensor, cj: float = 1.0, ck: float = -0.5, out: torch.Tensor | None = None,
+                     stream=None) -> torch.Tensor:
+        """sum_ijkl Gamma_ijkl d(ij|kl)/dR with Gamma = cj D_ij D_kl + ck D_ik D_jl (3N vector)."""
+        D = D.to(device=self.device, dtype=torch.float64).contiguous()
+        if out is None:
+            out = torch.empty(3 * self.natom, dtype=torch.float64, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.check(
+                _lib.load().qx_grad_adjoint(self.handle, C.c_void_p(D.data_ptr()), float(cj), float(ck),
+                                            C.c_void_p(out.data_ptr()), 1, C.c_void_p(_stream_ptr(stream))),
+                "qx_grad_adjoint",
+            )
+        return out
