@@ -1,0 +1,395 @@
+#!/usr/bin/env python3
+"""Headline benchmark: FP64 electron-repulsion integrals on B200.
+
+Workload (one "step"): every Schwarz-screened 8-fold-unique contracted shell
+quartet of a seeded synthetic molecule -- 10 atoms uniform in a 12-bohr cube
+(minimum separation 1.8 bohr), Z in {1,6,8}, heavy atoms s,s,s,p,p,d and H s,s,p,
+K ~ U{1..8} primitives per shell, exponents log-uniform in [0.08, 5e3], Schwarz
+threshold 1e-12, Cartesian shells (the reference's convention) -- evaluated in
+FP64 through the library's device path, with inputs resident in HBM.
+
+  value   unique quartets / s over all ranks (replicas: one molecule per GPU)
+  e2e     the same through the reference-facing C ABI with host buffers:
+          qx_initialize (shells H2D) -> qx_compute_2e_int into pinned host memory
+          (dense n^4 D2H, the reference's return convention) -> qx_finalize
+  extras  the HF-style geometric gradient sum Gamma dG of the same molecule by the
+          adjoint kernel and by the plain path (materialise the (3N,n^4) tensor,
+          then contract), seconds per evaluation
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Under torchrun (N>1) each rank runs its own replica; the max over ranks is used.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "HF geom-gradient s/eval (adjoint vs plain ERI-deriv) at 1e-8 Eh/bohr; quartets/s"
+WORKLOAD = "eri10"
+THR = 1e-12
+
+
+def workload_desc(b, extra=None):
+    d = {
+        "workload": "10-atom synthetic molecule, l<=2, K 1-8, Schwarz 1e-12, full unique FP64 ERI (seed 0)",
+        "natom": b.natom,
+        "nshell": b.nshell,
+        "nbf": b.nbf(),
+        "shells": "cartesian",
+        "schwarz_tol": THR,
+        "l2": "flushed between steps (256 MiB write); inputs are L2-resident pair data",
+        "parallelism": "replicas (one molecule per GPU, no exchange)",
+    }
+    if extra:
+        d.update(extra)
+    return d
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+# ------------------------------------------------------------------ clocks ----
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.f = None
+
+    def __enter__(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms",
+                 "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or self.f is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for ln in fh:
+                p = [x.strip() for x in ln.split(",")]
+                if len(p) >= 9:
+                    rows.append(p)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------------ our arm ---
+def fp64_peak_tflops():
+    lib = ctypes.CDLL(os.path.join(ROOT, "quax_b200", "libqx_peaks.so"))
+    lib.qx_fma_peak_tflops.restype = ctypes.c_double
+    lib.qx_fma_peak_tflops.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.qx_fma_peak_tflops(1, 2000, 1)
+    return max(lib.qx_fma_peak_tflops(1, 20000, 3) for _ in range(3))
+
+
+def cpu_baseline_eri(basis, target_s=12.0):
+    """Oracle (CPU port, all host threads) on a bounded sample of the same quartets."""
+    from oracle import api
+
+    ob = api.OracleBasis(basis)
+    K, kmax = api.schwarz(ob)
+    # calibrate: a small sample, then a sample sized for ~target_s seconds
+    t = time.perf_counter()
+    n0, _ = api.unique_sample(ob, THR, 400, 0, K=K, kmax=kmax)
+    dt0 = max(time.perf_counter() - t, 1e-3)
+    rate0 = n0 / dt0
+    total = api.count_unique(ob, THR)
+    stride = max(1, int(total / max(rate0 * target_s, 1.0)))
+    t = time.perf_counter()
+    n, _ = api.unique_sample(ob, THR, stride, 1 % stride, K=K, kmax=kmax)
+    dt = time.perf_counter() - t
+    return {"value": n / dt, "unit": "quartets/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"every {stride}-th of {total} screened unique quartets ({n} quartets, {dt:.1f} s; "
+                      f"Schwarz pass excluded); C/OpenMP oracle, FP64"}
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    from quax_b200.basis import config_spec, synthetic_molecule
+    from quax_b200.integrals import _lib
+    from quax_b200.integrals.engine import EriEngine
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    mol, b = synthetic_molecule(config_spec(WORKLOAD), 0)
+    eng = EriEngine(b, THR)
+    nq = eng.unique_quartets()
+    out = torch.empty(eng.unique_size(), dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    info = eng.class_info()
+    total_flops = sum(c["flops"] for c in info)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        eng.eri_unique(out)
+    barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        barrier()
+        for s in range(args.steps):
+            flush.zero_()
+            ev[s][0].record()
+            eng.eri_unique(out)
+            ev[s][1].record()
+        barrier()
+    clocks = clk.summary()
+    ms = sum(a.elapsed_time(b_) for a, b_ in ev)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    value = world * nq / (ms_per_step * 1e-3)
+    launches = sum(1 for c in info if c["nq"] > 0) * args.steps
+
+    # roofline of the dominant kernel: time every class launch alone (events on the
+    # launching stream), pick the longest, FLOPs from the op-count table
+    s = torch.cuda.current_stream()
+    per = []
+    for c in info:
+        if c["nq"] == 0:
+            continue
+        eng.eri_unique_class(c["cls"], out)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        reps = 3
+        e0.record(s)
+        for _ in range(reps):
+            eng.eri_unique_class(c["cls"], out)
+        e1.record(s)
+        torch.cuda.synchronize()
+        per.append((e0.elapsed_time(e1) / reps, c))
+    per.sort(key=lambda x: -x[0])
+    dom_ms, dom = per[0]
+    peak = fp64_peak_tflops()
+    achieved = dom["flops"] / (dom_ms * 1e-3) / 1e12
+    roofline = {
+        "bound": "fp64",
+        "kernel": f"class ({dom['l'][0]}{dom['l'][1]}|{dom['l'][2]}{dom['l'][3]}) ERI kernel",
+        "achieved": achieved,
+        "peak": peak,
+        "unit": "TFLOP/s",
+        "frac": achieved / peak if peak > 0 else None,
+        "peak_source": "measured FP64 FMA probe (libqx_peaks.so), not in MEASURED_PEAKS.json",
+        "traffic": None,
+        "step_achieved_tflops": total_flops / (ms_per_step * 1e-3) / 1e12,
+        "dominant_share_of_serial_sum": dom_ms / sum(p[0] for p in per),
+    }
+
+    # end to end through the reference-facing C ABI with host buffers
+    lib = _lib.load()
+    fl = b.flat()
+    coords = np.ascontiguousarray(b.atom_coords().reshape(-1))
+    n = eng.nbf
+    host = torch.empty(n**4, dtype=torch.float64, pin_memory=True)
+    h2d = coords.nbytes + sum(fl[k].nbytes for k in ("l", "nprim", "atom", "exps", "coefs"))
+
+    def e2e_step():
+        h = ctypes.c_void_p()
+        _lib.check(lib.qx_initialize(b.natom, _lib.dptr(coords), b.nshell, _lib.iptr(fl["l"]), _lib.iptr(fl["nprim"]),
+                                     _lib.iptr(fl["atom"]), _lib.dptr(fl["exps"]), _lib.dptr(fl["coefs"]), 0, THR,
+                                     ctypes.byref(h)), "qx_initialize")
+        _lib.check(lib.qx_compute_2e_int(h, ctypes.c_void_p(host.data_ptr()), 0, ctypes.c_void_p(0)),
+                   "qx_compute_2e_int")
+        lib.qx_finalize(h)
+
+    e2e_step()
+    barrier()
+    t0 = time.perf_counter()
+    e2e_steps = max(1, min(args.steps, 3))
+    for _ in range(e2e_steps):
+        e2e_step()
+    barrier()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    e2e = {"value": world * nq / e2e_s, "unit": "quartets/s", "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(8 * n**4), "ms_per_step": e2e_s * 1e3,
+           "path": "qx_initialize + qx_compute_2e_int(host pinned n^4) + qx_finalize"}
+    del host
+
+    grad = None
+    if not args.no_grad:
+        grad = gradient_extras(eng, b, n, args.warmup)
+
+    cpu = cpu_baseline_eri(b) if rank == 0 else None
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "quartets/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_per_step,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic (seeded generator; no dataset)",
+            "config": workload_desc(b, {"unique_quartets": nq, "primitive_quartets": sum(c["prims"] for c in info)}),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "gradient": grad,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def gradient_extras(eng, b, n, warmup):
+    """Adjoint vs plain gradient sum Gamma dG (HF Gamma from a random density)."""
+    import numpy as np
+    import torch
+
+    rng = np.random.default_rng(0)
+    C = rng.normal(0.0, 1.0 / np.sqrt(n), size=(n, n // 4))
+    D = torch.from_numpy(C @ C.T).cuda()
+    for _ in range(max(1, warmup)):
+        g = eng.grad_adjoint(D)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 3
+    e0.record()
+    for _ in range(reps):
+        g = eng.grad_adjoint(D)
+    e1.record()
+    torch.cuda.synchronize()
+    adj_s = e0.elapsed_time(e1) / reps * 1e-3
+    out = {"adjoint_s": adj_s, "plain_s": None, "max_abs_diff_Eh_per_bohr": None,
+           "gamma": "cj D_ij D_kl + ck D_ik D_jl, cj=1, ck=-1/2, D = C C^T, C n x n/4 N(0,1/n)"}
+    need = 8 * (3 * b.natom * n**4 + n**4)
+    free, _ = torch.cuda.mem_get_info()
+    if need < 0.9 * free:
+        dG = torch.empty((3 * b.natom, n, n, n, n), dtype=torch.float64, device="cuda")
+        Gam = torch.einsum("ij,kl->ijkl", D, D) - 0.5 * torch.einsum("ik,jl->ijkl", D, D)
+        eng.eri_deriv_core(out=dG)
+        torch.cuda.synchronize()
+        e0.record()
+        eng.eri_deriv_core(out=dG)
+        gv = Gam.view(-1)
+        gp = torch.stack([torch.dot(dG[x].view(-1), gv) for x in range(3 * b.natom)])
+        e1.record()
+        torch.cuda.synchronize()
+        out["plain_s"] = e0.elapsed_time(e1) * 1e-3
+        out["max_abs_diff_Eh_per_bohr"] = float((gp - g).abs().max())
+        out["adjoint_speedup_vs_plain"] = out["plain_s"] / adj_s
+        del dG, Gam
+        torch.cuda.empty_cache()
+    else:
+        out["plain_s"] = f"skipped: needs {need / 1e9:.0f} GB"
+    return out
+
+
+# ------------------------------------------------------------- reference arm ---
+def run_reference(args):
+    """The reference's CPU path for this workload on the host cores.  Libint (the
+    reference's engine) cannot be built or imported on this image, so the timed CPU
+    implementation is the oracle port (C/OpenMP restatement of the same algorithm
+    and screening), each step a bounded sample of the workload."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import api
+    from quax_b200.basis import config_spec, synthetic_molecule
+
+    mol, b = synthetic_molecule(config_spec(WORKLOAD), 0)
+    ob = api.OracleBasis(b)
+    K, kmax = api.schwarz(ob)
+    total = api.count_unique(ob, THR)
+    stride = 64
+    for w in range(args.warmup):
+        api.unique_sample(ob, THR, stride * 4, w % (stride * 4), K=K, kmax=kmax)
+    t = time.perf_counter()
+    done = 0
+    for s in range(args.steps):
+        n, _ = api.unique_sample(ob, THR, stride, s % stride, K=K, kmax=kmax)
+        done += n
+    dt = time.perf_counter() - t
+    value = done / dt
+    sample = (f"each step: every {stride}-th of {total} screened unique quartets (phase = step index); "
+              f"{done} quartets in {dt:.1f} s; Schwarz pass excluded; oracle C/OpenMP port (Libint unavailable)")
+    line = {
+        "metric": METRIC, "value": value, "unit": "quartets/s", "impl": "reference", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator; no dataset)",
+        "config": workload_desc(b, {"unique_quartets": total}),
+        "cpu_baseline": {"value": value, "unit": "quartets/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "quartets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-grad", action="store_true", help="skip the adjoint/plain gradient extras")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -120,6 +120,18 @@ int qx_compute_2e_deriv(qx_handle *h, const int *deriv_vec, int len, double *out
 int qx_grad_adjoint(qx_handle *h, const double *D, double cj, double ck, double *grad, int on_device,
                     void *stream);
 
+/* Angular-momentum classes (canonical (la lb|lc ld), la>=lb, lc>=ld, bra class >=
+ * ket class) and per-class work of a handle: screened unique quartets, primitive
+ * quartets, and algorithmic FP64 FLOPs of the plain and first-derivative programs
+ * (counting rule in quax_b200/csrc/gen_eri.py).  No counterpart in the reference;
+ * used for roofline accounting and per-class timing. */
+int qx_num_classes(void);
+int qx_class_info(const qx_handle *h, int cls, int *l4, long long *nquartets, long long *nprim_quartets,
+                  double *flops, double *flops_deriv);
+
+/* qx_eri_unique restricted to one class (same output positions). */
+int qx_eri_unique_class(qx_handle *h, int cls, double *out_dev, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -55,7 +55,8 @@ def lib():
         L.qxo_eri_deriv1.argtypes = [C.POINTER(_Basis), C.c_double, C.c_int, _dp, C.c_int]
         L.qxo_grad_contract.argtypes = [C.POINTER(_Basis), C.c_double, _dp, C.c_double, C.c_double, _dp, C.c_int]
         L.qxo_unique_sample.restype = C.c_long
-        L.qxo_unique_sample.argtypes = [C.POINTER(_Basis), C.c_double, C.c_long, C.c_long, C.c_int, _dp, C.c_int]
+        L.qxo_unique_sample.argtypes = [C.POINTER(_Basis), C.c_double, C.c_long, C.c_long, C.c_int, _dp, C.c_double,
+                                        _dp, C.c_int]
         L.qxo_count_unique.restype = C.c_long
         L.qxo_count_unique.argtypes = [C.POINTER(_Basis), C.c_double, C.c_int]
         L.qxo_how_many_derivs.argtypes = [C.c_int, C.c_int]
@@ -158,9 +159,14 @@ def grad_contract(ob: OracleBasis, thr: float, D: np.ndarray, cj=1.0, ck=-0.5, n
     return g
 
 
-def unique_sample(ob: OracleBasis, thr: float, stride: int, phase: int = 0, deriv=False, nthreads: int = 0):
+def unique_sample(ob: OracleBasis, thr: float, stride: int, phase: int = 0, deriv=False, nthreads: int = 0,
+                  K=None, kmax: float = 0.0):
+    """Evaluate every stride-th screened unique quartet; K/kmax from schwarz() skip the
+    screening pass so only quartet work is timed."""
     cs = C.c_double()
-    n = lib().qxo_unique_sample(ob.ref, thr, int(stride), int(phase), int(bool(deriv)), C.byref(cs), nthreads)
+    Kp = _p(np.ascontiguousarray(K, dtype=np.float64)) if K is not None else None
+    n = lib().qxo_unique_sample(ob.ref, thr, int(stride), int(phase), int(bool(deriv)), Kp, float(kmax), C.byref(cs),
+                                nthreads)
     return n, cs.value
 
 

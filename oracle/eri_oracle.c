@@ -693,16 +693,22 @@ int qxo_grad_contract(const qxo_basis *B, double thr, const double *Dm, double c
 /* Time-bounded unique-quartet evaluation for the CPU baseline: evaluates the
  * screened 8-fold-unique quartets whose linear index (in bra-major, ket <= bra
  * order over the reference pair list) is congruent to `phase` modulo `stride`,
- * discarding results; returns the number of quartets evaluated.  deriv selects
+ * discarding results; returns the number of quartets evaluated.  K_in (the Schwarz
+ * table of qxo_schwarz) may be passed so the call times quartet work only.  deriv selects
  * the first-derivative engine.  checksum receives a sum of the first element of
  * every block so the work cannot be optimised away. */
-long qxo_unique_sample(const qxo_basis *B, double thr, long stride, long phase, int deriv,
-                       double *checksum, int nthreads) {
+long qxo_unique_sample(const qxo_basis *B, double thr, long stride, long phase, int deriv, const double *K_in,
+                       double kmax_in, double *checksum, int nthreads) {
     init_tables();
     int ns = B->nshell;
     double *K = (double *)malloc(sizeof(double) * ns * ns);
     double kmax;
-    qxo_schwarz(B, K, &kmax, nthreads);
+    if (K_in) {
+        memcpy(K, K_in, sizeof(double) * ns * ns);
+        kmax = kmax_in;
+    } else {
+        qxo_schwarz(B, K, &kmax, nthreads);
+    }
     int *pairs = (int *)malloc(sizeof(int) * ns * (ns + 1));
     int np = qxo_pairs(B, K, kmax, thr, pairs);
     double thr2 = thr * thr;

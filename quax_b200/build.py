@@ -21,6 +21,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libquax_b200.so")
+PEAKS_LIB = os.path.join(PKG, "libqx_peaks.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + [
     "-lineinfo",
@@ -78,13 +79,20 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
     with ThreadPoolExecutor(max_workers=jobs or os.cpu_count() or 4) as ex:
         results = list(ex.map(lambda s: _compile(s, hmt, verbose), srcs))
     objs = [o for o, _ in results]
-    rebuilt = any(b for _, b in results)
-    if rebuilt or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
-        cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs
+    _link(LIB, objs, any(b for _, b in results))
+    # FMA throughput probe used by the benchmark's roofline (separate library)
+    psrc = os.path.join(CSRC, "peaks", "qx_peaks.cu")
+    pobj, pb = _compile(psrc, hmt, verbose)
+    _link(PEAKS_LIB, [pobj], pb)
+    return LIB
+
+
+def _link(lib: str, objs, rebuilt: bool):
+    if rebuilt or not os.path.exists(lib) or os.path.getmtime(lib) < max(os.path.getmtime(o) for o in objs):
+        cmd = [nvcc()] + ARCH + ["-shared", "-o", lib] + objs
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
-    return LIB
 
 
 if __name__ == "__main__":

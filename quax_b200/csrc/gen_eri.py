@@ -434,7 +434,7 @@ def coop_program(la, lb, lc, ld):
     targets = [vd.get(e, f, 0) for e, f in acc.targets()]
     vnodes = sorted(vd.nodes, key=lambda n: n[-1])
     vlev = []
-    for lv in range(1, max(n[-1] for n in vnodes) + 1):
+    for lv in range(1, max((n[-1] for n in vnodes), default=0) + 1):
         vlev.append(sum(1 for n in vnodes if n[-1] < lv))
     vlev.append(len(vnodes))
     hd = HRRDag(acc)
@@ -660,6 +660,30 @@ def gen_coop_deriv(classes):
     return "\n".join(lines) + "\n"
 
 
+# ----------------------------------------------------------------------------------
+# Algorithmic FLOP counts (the roofline's work unit).  Counting rule, fixed:
+#   VRR node: c1*x + c2*y = 3; the e_i/(2 zeta) term +4; the coupling term +2;
+#   target accumulation 1 (plain) / 2 (weighted derivative sets);
+#   primitive set-up (P-Q geometry, Boys Taylor + downward recursion, exp) 60;
+#   HRR node 2 per contracted quartet (identity copies 0).
+# ----------------------------------------------------------------------------------
+SETUP_FLOPS = 60
+
+
+def vrr_node_flops(k, ne):
+    return 3 + (4 if k else 0) + (2 if ne else 0)
+
+
+def class_flops(la, lb, lc, ld):
+    p = coop_program(la, lb, lc, ld)
+    vrr = SETUP_FLOPS + sum(vrr_node_flops(n[8], n[9]) for n in p["vnodes"]) + len(p["targets"])
+    hrr = 2 * len(p["hnodes"])
+    d = coop_deriv_program(la, lb, lc, ld)
+    dvrr = SETUP_FLOPS + sum(vrr_node_flops(n[8], n[9]) for n in d["vnodes"]) + 2 * len(d["targets"])
+    dhrr = 2 * sum(1 for n in d["hnodes"] if n[3] != 3)
+    return vrr, hrr, dvrr, dhrr
+
+
 def pair_classes(lmax):
     return [(a, b) for a in range(lmax + 1) for b in range(a + 1)]
 
@@ -679,6 +703,8 @@ def main():
     os.makedirs(os.path.join(here, "gen"), exist_ok=True)
     hdr = [
         "// Generated by quax_b200/csrc/gen_eri.py -- do not edit by hand.",
+        "// QX_CLASS_*_FLOPS: VRR per primitive quartet, HRR per contracted quartet",
+        "// (plain and first-derivative programs; counting rule in gen_eri.py).",
         f"// Canonical classes up to l = {lmax}.",
         "#pragma once",
         f"#define QX_GEN_LMAX {lmax}",
@@ -694,6 +720,9 @@ def main():
     hdr.append("#define QX_CLASS_COOP " + "{" + ", ".join("1" if c in COOP_CLASSES else "0" for c in qc) + "}")
     hdr.append("// X(class_id, LA, LB, LC, LD) for the classes with straight-line kernels")
     hdr.append("#define QX_FOR_EACH_SL_CLASS(X) " + " ".join(f"X({i}, {a}, {b}, {c}, {d})" for i, (a, b, c, d) in enumerate(qc) if (a, b, c, d) not in COOP_CLASSES))
+    fl = [class_flops(*c) for c in qc]
+    for k, name in enumerate(("VRR", "HRR", "DVRR", "DHRR")):
+        hdr.append(f"#define QX_CLASS_{name}_FLOPS " + "{" + ", ".join(str(f[k]) for f in fl) + "}")
     body = [gen_plain(*c) for c in qc if c not in COOP_CLASSES]
     with open(os.path.join(here, "gen", "coop_tables.cuh"), "w") as f:
         f.write(gen_coop([(i, c) for i, c in enumerate(qc) if c in COOP_CLASSES]))

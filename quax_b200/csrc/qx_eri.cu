@@ -74,6 +74,15 @@ static EriLaunch g_eri_launch[QX_NUM_CLASSES];
 static long long g_class_scratch[QX_NUM_CLASSES];
 static const int g_class_nout[QX_NUM_CLASSES] = QX_CLASS_NOUT;
 static const int g_class_coop[QX_NUM_CLASSES] = QX_CLASS_COOP;
+static const long long g_class_vrr_flops[QX_NUM_CLASSES] = QX_CLASS_VRR_FLOPS;
+static const long long g_class_hrr_flops[QX_NUM_CLASSES] = QX_CLASS_HRR_FLOPS;
+static const long long g_class_dvrr_flops[QX_NUM_CLASSES] = QX_CLASS_DVRR_FLOPS;
+static const long long g_class_dhrr_flops[QX_NUM_CLASSES] = QX_CLASS_DHRR_FLOPS;
+static const int g_class_l[QX_NUM_CLASSES][4] = {
+#define QX_L_ENTRY(id, a, b, c, d) {a, b, c, d},
+    QX_FOR_EACH_CLASS(QX_L_ENTRY)
+#undef QX_L_ENTRY
+};
 static int g_coop_idx[QX_NUM_CLASSES];
 static int g_der_idx[QX_NUM_CLASSES];
 
@@ -672,4 +681,29 @@ extern "C" int qx_grad_adjoint(qx_handle* h, const double* D, double cj, double 
     cudaFree(dg);
     if (!rc) rc = check_err_word(h, s);
     return rc;
+}
+
+// ---------------------------------------------------------------- class info ---
+extern "C" int qx_num_classes(void) { return QX_NUM_CLASSES; }
+
+extern "C" int qx_class_info(const qx_handle* h, int cls, int* l4, long long* nquartets, long long* nprim_quartets,
+                             double* flops, double* flops_deriv) {
+    if (!h || cls < 0 || cls >= QX_NUM_CLASSES) return fail(QX_E_INVALID, "qx_class_info: bad handle or class");
+    const ClassWork& w = h->work[cls];
+    if (l4)
+        for (int i = 0; i < 4; ++i) l4[i] = g_class_l[cls][i];
+    if (nquartets) *nquartets = w.nq;
+    if (nprim_quartets) *nprim_quartets = w.prims;
+    if (flops) *flops = (double)w.prims * g_class_vrr_flops[cls] + (double)w.nq * g_class_hrr_flops[cls];
+    if (flops_deriv) *flops_deriv = (double)w.prims * g_class_dvrr_flops[cls] + (double)w.nq * g_class_dhrr_flops[cls];
+    return QX_OK;
+}
+
+extern "C" int qx_eri_unique_class(qx_handle* h, int cls, double* out_dev, void* stream) {
+    if (!h || !out_dev || cls < 0 || cls >= QX_NUM_CLASSES) return fail(QX_E_INVALID, "qx_eri_unique_class: bad argument");
+    DeviceGuard g(h->device);
+    const ClassWork& w = h->work[cls];
+    if (!w.nq) return QX_OK;
+    return run_class(h, cls, MODE_UNIQUE, w.d_q, w.nq, out_dev, 0, w.unique_base, (cudaStream_t)stream, w.log2g,
+                     w.scratch);
 }

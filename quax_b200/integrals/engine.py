@@ -81,6 +81,21 @@ class EriEngine:
         _lib.check(_lib.load().qx_schwarz(self.handle, _lib.dptr(K), C.byref(kmax)), "qx_schwarz")
         return K, kmax.value
 
+    def class_info(self):
+        """Per angular-momentum class: (la,lb,lc,ld), quartets, primitive quartets,
+        plain FLOPs, first-derivative FLOPs."""
+        lib = _lib.load()
+        out = []
+        for c in range(lib.qx_num_classes()):
+            l4 = np.zeros(4, dtype=np.int32)
+            nq, npq = C.c_longlong(), C.c_longlong()
+            f, fd = C.c_double(), C.c_double()
+            _lib.check(lib.qx_class_info(self.handle, c, _lib.iptr(l4), C.byref(nq), C.byref(npq), C.byref(f),
+                                         C.byref(fd)), "qx_class_info")
+            out.append(dict(cls=c, l=tuple(int(x) for x in l4), nq=nq.value, prims=npq.value, flops=f.value,
+                            flops_deriv=fd.value))
+        return out
+
     # -- integrals ------------------------------------------------------------
     def eri(self, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
         """Dense (n,n,n,n) FP64 ERI tensor on the device (reference layout)."""
@@ -113,6 +128,15 @@ class EriEngine:
             _lib.check(
                 _lib.load().qx_eri_unique(self.handle, C.c_void_p(out.data_ptr()), C.c_void_p(_stream_ptr(stream))),
                 "qx_eri_unique",
+            )
+        return out
+
+    def eri_unique_class(self, cls: int, out: torch.Tensor, stream=None) -> torch.Tensor:
+        with torch.cuda.device(self.device):
+            _lib.check(
+                _lib.load().qx_eri_unique_class(self.handle, int(cls), C.c_void_p(out.data_ptr()),
+                                                C.c_void_p(_stream_ptr(stream))),
+                "qx_eri_unique_class",
             )
         return out
 
