@@ -132,6 +132,29 @@ int qx_class_info(const qx_handle *h, int cls, int *l4, long long *nquartets, lo
 /* qx_eri_unique restricted to one class (same output positions). */
 int qx_eri_unique_class(qx_handle *h, int cls, double *out_dev, void *stream);
 
+/* Size of the fixed device array qx_compute_2e_int_noalloc works in. */
+#define QX_NOALLOC_SCRATCH_BYTES (16u << 20)
+
+/* Dense ERI tensor for callers that cannot allocate device memory.  No counterpart
+ * in the reference: it exists for hosts where the library must not call cudaMalloc,
+ * such as an XLA/JAX custom call (the runtime owns and pre-reserves the device
+ * memory), real-time hosts that forbid allocation after start-up, and code that
+ * accounts for every device byte in its own pool.  It computes what
+ * qx_initialize + qx_compute_2e_int + qx_finalize compute (same arguments as
+ * qx_initialize, Cartesian shells, out_dev = n^4 doubles of caller-owned device
+ * memory) but keeps every internal table in one static device array of
+ * QX_NOALLOC_SCRATCH_BYTES, held on every device that uses it until the process
+ * exits.  It calls no cudaMalloc/cudaFree, creates no streams, runs on `stream` and
+ * returns when the tensor is complete.  A basis whose tables do not fit (about
+ * 1.5 million screened unique quartets) is rejected with QX_E_INVALID.  All calls
+ * share the array, which keeps the previous call's contents, so calls that overlap
+ * on the GPU race and must be serialised by the caller.  The first call on a device
+ * looks up the array's address and uploads a constant table synchronously; make it
+ * before any stream capture.  Errors are reported through qx_last_error(). */
+int qx_compute_2e_int_noalloc(int natom, const double *coords, int nshell, const int *shell_l,
+                              const int *shell_nprim, const int *shell_atom, const double *exps,
+                              const double *coefs, double ints_tol, double *out_dev, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -49,6 +49,7 @@ static int fail(int code, const char* fmt, ...) {
     } while (0)
 
 extern "C" const char* qx_last_error(void) { return g_err.c_str(); }
+void qx_set_last_error(const char* msg) { g_err = msg; }
 extern "C" int qx_max_l(void) { return QX_GEN_LMAX; }
 extern "C" int qx_max_deriv_order(void) { return 1; }
 
