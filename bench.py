@@ -194,6 +194,13 @@ def run_ours(args):
     value = world * nq / (ms_per_step * 1e-3)
     launches = sum(1 for c in info if c["nq"] > 0) * args.steps
 
+    if args.no_extras:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": "quartets/s", "ms_per_step": ms_per_step,
+                              "note": "--no-extras (profiling run)"}), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     # roofline of the dominant kernel: time every class launch alone (events on the
     # launching stream), pick the longest, FLOPs from the op-count table
     s = torch.cuda.current_stream()
@@ -382,6 +389,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-grad", action="store_true", help="skip the adjoint/plain gradient extras")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="time the ERI steps only (for profiler runs): no roofline probe, e2e, gradient or CPU arm")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
