@@ -342,6 +342,32 @@ def gradient_extras(eng, b, n, warmup):
     return out
 
 
+def run_grad_only(args):
+    """Adjoint gradient of the workload only (profiling aid; prints its timing)."""
+    import numpy as np
+    import torch
+
+    from quax_b200.basis import config_spec, synthetic_molecule
+    from quax_b200.integrals.engine import EriEngine
+
+    mol, b = synthetic_molecule(config_spec(WORKLOAD), 0)
+    eng = EriEngine(b, THR)
+    n = eng.nbf
+    rng = np.random.default_rng(0)
+    C = rng.normal(0.0, 1.0 / np.sqrt(n), size=(n, n // 4))
+    D = torch.from_numpy(C @ C.T).cuda()
+    for _ in range(args.warmup):
+        eng.grad_adjoint(D)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        eng.grad_adjoint(D)
+    e1.record()
+    torch.cuda.synchronize()
+    print(json.dumps({"adjoint_ms": e0.elapsed_time(e1) / args.steps, "note": "--profile-grad"}), flush=True)
+
+
 # ------------------------------------------------------------- reference arm ---
 def run_reference(args):
     """The reference's CPU path for this workload on the host cores.  Libint (the
@@ -389,6 +415,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-grad", action="store_true", help="skip the adjoint/plain gradient extras")
+    ap.add_argument("--profile-grad", action="store_true",
+                    help="run only the adjoint gradient of the workload, warmup+steps times (for profiler runs)")
     ap.add_argument("--no-extras", action="store_true",
                     help="time the ERI steps only (for profiler runs): no roofline probe, e2e, gradient or CPU arm")
     args = ap.parse_args()
@@ -396,6 +424,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.profile_grad:
+        run_grad_only(args)
     else:
         run_ours(args)
 

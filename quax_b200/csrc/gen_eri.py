@@ -548,8 +548,12 @@ class HRRMulti:
             i = first_dir(b)
             dst = self._new(self.get(sp, sh(a, i, 1), sh(b, i, -1), c, d), self.get(sp, a, sh(b, i, -1), c, d), 0, i)
         else:
-            acc, off = self.spaces[sp]
-            dst = off + acc.index(a, c)
+            lm = getattr(self, "leafmap", None)
+            if lm is not None:
+                dst = lm[(sp, a, c)]
+            else:
+                acc, off = self.spaces[sp]
+                dst = off + acc.index(a, c)
         self.slot[key] = dst
         return dst
 
@@ -684,6 +688,168 @@ def class_flops(la, lb, lc, ld):
     return vrr, hrr, dvrr, dhrr
 
 
+# ----------------------------------------------------------------------------------
+# Warp-per-quartet kernels (qx_warp.cuh): lanes = primitive quartets.  The class's
+# straight-line VRR runs in each lane; its targets become "items" in emission
+# order (derivative targets once per accumulator set, times the set weight), which
+# are staged 16 at a time and folded across the warp by reduce16 into the warp's
+# shared accumulators.  The HRR tables are built over that item order.
+# ----------------------------------------------------------------------------------
+WARP_PEAK_MAX = 400  # VRR values a lane may keep live (registers, spills to L1 beyond)
+
+
+def _warp_targets(la, lb, lc, ld, deriv):
+    lab, lcd = la + lb, lc + ld
+    if not deriv:
+        acc = AccSpace("acc", la, lab, lc, lcd)
+        return [((e, f), ["acc"]) for e, f in reversed(list(acc.targets()))], {"acc": acc}
+    spaces = {"U": AccSpace("U", la - 1, lab, lc - 1, lcd), "WA": AccSpace("WA", la + 1, lab + 1, lc, lcd),
+              "WB": AccSpace("WB", la, lab + 1, lc, lcd), "WC": AccSpace("WC", la, lab, lc + 1, lcd + 1)}
+    member = {}
+    for name in ("U", "WA", "WB", "WC"):
+        for t in spaces[name].targets():
+            member.setdefault(t, []).append(name)
+    order = sorted(member, key=lambda t: (-sum(t[0]), -sum(t[1]), gidx(t[0]), gidx(t[1])))
+    return [(t, member[t]) for t in order], spaces
+
+
+def _peak_live(lines, consumed_at):
+    """Peak live count of SSA values in `lines` (values die at their last use)."""
+    import re as _re
+    uses = {}
+    defs = []
+    for i, ln in enumerate(lines):
+        m = _re.match(r"const double (v\d+) = (.*);", ln)
+        body = m.group(2) if m else ln
+        for d in _re.findall(r"\b(v\d+)\b", body):
+            uses[d] = i
+        defs.append(m.group(1) if m else None)
+    alive, pk = set(), 0
+    for i, ln in enumerate(lines):
+        if defs[i]:
+            alive.add(defs[i])
+            pk = max(pk, len(alive))
+        for d in list(alive):
+            if uses.get(d, -1) <= i and d != defs[i]:
+                alive.discard(d)
+    return pk
+
+
+def warp_program(la, lb, lc, ld, deriv):
+    S = la + lb + lc + ld + (1 if deriv else 0)
+    tlist, spaces = _warp_targets(la, lb, lc, ld, deriv)
+    em = Emitter("v")
+    vr = VRR(em)
+    items = []  # (space, e, f)
+    leaf = {}
+    wname = {"acc": None, "U": None, "WA": "wa", "WB": "wb", "WC": "wc"}
+    for (e, f), sets in tlist:
+        v = vr.get(e, f, 0)
+        for sp in sets:
+            k = len(items)
+            items.append((sp, e, f))
+            leaf[(sp, e, f)] = k
+            w = wname[sp]
+            em.lines.append(f"stg[{k % 16}] = {v};" if w is None else f"stg[{k % 16}] = {w} * {v};")
+            if k % 16 == 15:
+                em.lines.append(f"reduce16(stg, acc + {k - 15}, lane);")
+    nitem = len(items)
+    if nitem % 16:
+        for k in range(nitem, (nitem + 15) // 16 * 16):
+            em.lines.append(f"stg[{k % 16}] = 0.0;")
+        em.lines.append(f"reduce16(stg, acc + {(nitem // 16) * 16}, lane);")
+    nitem_pad = (nitem + 15) // 16 * 16
+    peak = _peak_live(em.lines, None)
+    # HRR over the item layout
+    nout = ncart(la) * ncart(lb) * ncart(lc) * ncart(ld)
+    if not deriv:
+        hm = HRRMulti({"acc": (spaces["acc"], 0)})
+        hm.next = nitem_pad
+        hm.leafmap = leaf
+        outs = [hm.get("acc", a, b, c, d) for a in comps(la) for b in comps(lb) for c in comps(lc) for d in comps(ld)]
+        hnodes = sorted(hm.nodes, key=lambda n: n[-1])
+        hout = None
+        pinned = outs
+    else:
+        hm = HRRMulti({k: (v, 0) for k, v in spaces.items()})
+        hm.next = nitem_pad
+        hm.leafmap = leaf
+        outs = [None] * (9 * nout)
+        kk = 0
+        for a in comps(la):
+            for b in comps(lb):
+                for c in comps(lc):
+                    for d in comps(ld):
+                        for i in range(3):
+                            x = hm.get("WA", sh(a, i, 1), b, c, d)
+                            outs[i * nout + kk] = hm.combine(x, hm.get("U", sh(a, i, -1), b, c, d), a[i]) if a[i] else x
+                            x = hm.get("WB", a, sh(b, i, 1), c, d)
+                            outs[(3 + i) * nout + kk] = hm.combine(x, hm.get("U", a, sh(b, i, -1), c, d), b[i]) if b[i] else x
+                            x = hm.get("WC", a, b, sh(c, i, 1), d)
+                            outs[(6 + i) * nout + kk] = hm.combine(x, hm.get("U", a, b, sh(c, i, -1), d), c[i]) if c[i] else x
+                        kk += 1
+        owner = {}
+        for ob, sl in enumerate(outs):
+            if sl < nitem_pad or sl in owner:
+                sl = hm._new(sl, sl, 3, 0)
+                outs[ob] = sl
+            owner[sl] = ob
+        hnodes = sorted(hm.nodes, key=lambda n: n[-1])
+        hout = [owner.get(n[0], 0xFFFF) for n in hnodes]
+        pinned = []
+    hlev = [sum(1 for n in hnodes if n[-1] < lv) for lv in range(1, max((n[-1] for n in hnodes), default=0) + 1)]
+    hlev.append(len(hnodes))
+    hnodes2, pinned2, hslots = _realloc([(n[0], n[1:3], n[-1]) for n in hnodes], hnodes, pinned, nitem_pad, "h")
+    return dict(S=S, lines=em.lines, nitem=nitem, nitem_pad=nitem_pad, peak=peak, hnodes=hnodes2, hlev=hlev,
+                outs=pinned2 if not deriv else hout, hslots=max(hslots, nitem_pad), nout=nout)
+
+
+def warp_feasible(la, lb, lc, ld, deriv):
+    p = warp_program(la, lb, lc, ld, deriv)
+    return p["peak"] <= WARP_PEAK_MAX, p
+
+
+def gen_warp_code(cid, la, lb, lc, ld, deriv, p):
+    tag = f"{'d' if deriv else 'p'}{cid:02d}"
+    L = []
+    hn = [(dst | s1 << 16, s2 | side << 16 | dr << 18) for (dst, s1, s2, side, dr, lvl) in p["hnodes"]]
+    for n in hn:
+        assert n[0] < 2**32
+    def arr(name, typ, vals, per):
+        out = [f"static __device__ const {typ} {name}[{max(len(vals), 1)}] = {{"]
+        for i0 in range(0, len(vals), 8):
+            out.append("  " + ", ".join(per(v) for v in vals[i0:i0 + 8]) + ",")
+        if not vals:
+            out.append("  {}" if typ.startswith("uint") else "  0")
+        out.append("};")
+        return out
+    L += arr(f"k_hn_{tag}", "uint2", hn, lambda v: "{%du,%du}" % v)
+    L += arr(f"k_hl_{tag}", "int", p["hlev"], str)
+    outs = p["outs"]
+    L += arr(f"k_ho_{tag}", "unsigned short", outs, str)
+    extra = p["nout"] if deriv else 0
+    smem = p["hslots"] + 16 + extra
+    L.append(f"struct Warp_{tag} {{")
+    L.append(f"  static constexpr int LA = {la}, LB = {lb}, LC = {lc}, LD = {ld};")
+    L.append(f"  static constexpr int S = {p['S']}, NITEM = {p['nitem']}, NITEM_PAD = {p['nitem_pad']};")
+    L.append(f"  static constexpr int HSLOTS = {p['hslots']}, NOUT = {p['nout']}, NHLEV = {len(p['hlev']) - 1};")
+    L.append(f"  static constexpr int SMEM_PER_WARP = {smem};")
+    L.append(f"  static __device__ __forceinline__ const uint2* hnodes() {{ return k_hn_{tag}; }}")
+    L.append(f"  static __device__ __forceinline__ const int* hlev() {{ return k_hl_{tag}; }}")
+    L.append(f"  static __device__ __forceinline__ const unsigned short* outs() {{ return k_ho_{tag}; }}")
+    L.append("  template <class Q>")
+    L.append("  static __device__ __forceinline__ void vrr(const double* __restrict__ Fp, const Q& q, double wa, double wb,"
+             " double wc, double* __restrict__ acc, unsigned lane) {")
+    L.append("    (void)wa; (void)wb; (void)wc;")
+    L.append("    double stg[16];")
+    L += ["    " + ln for ln in p["lines"]]
+    L.append("  }")
+    L.append("};")
+    L.append(f"void qx_launch_warp_{tag}(const qx::WarpArgs& w, int mode, cudaStream_t s) "
+             f"{{ qx::launch_warp<Warp_{tag}, {1 if deriv else 0}>(w, mode, s); }}")
+    return "\n".join(L)
+
+
 def pair_classes(lmax):
     return [(a, b) for a in range(lmax + 1) for b in range(a + 1)]
 
@@ -718,6 +884,7 @@ def main():
     hdr.append(f"#define QX_NUM_PAIR_CLASSES {len(pair_classes(lmax))}")
     hdr.append("#define QX_CLASS_NOUT " + "{" + ", ".join(str(ncart(a) * ncart(b) * ncart(c) * ncart(d)) for (a, b, c, d) in qc) + "}")
     hdr.append("#define QX_CLASS_COOP " + "{" + ", ".join("1" if c in COOP_CLASSES else "0" for c in qc) + "}")
+    hdr.append("#define QX_CLASS_NACC {" + ", ".join(str(AccSpace("a", a, a + b, c, c + d).size) for (a, b, c, d) in qc) + "}")
     hdr.append("// X(class_id, LA, LB, LC, LD) for the classes with straight-line kernels")
     hdr.append("#define QX_FOR_EACH_SL_CLASS(X) " + " ".join(f"X({i}, {a}, {b}, {c}, {d})" for i, (a, b, c, d) in enumerate(qc) if (a, b, c, d) not in COOP_CLASSES))
     fl = [class_flops(*c) for c in qc]
@@ -731,14 +898,31 @@ def main():
     for fn in os.listdir(os.path.join(here, "gen")):
         if fn.startswith("k_eri_") and fn.endswith(".cu"):
             os.remove(os.path.join(here, "gen", fn))
+    wp, wd = [], []
     for i, (a, b, c, d) in enumerate(qc):
-        if (a, b, c, d) in COOP_CLASSES:
+        okp, pp = warp_feasible(a, b, c, d, 0)
+        okd, pd = warp_feasible(a, b, c, d, 1)
+        wp.append(okp)
+        wd.append(okd)
+        if (a, b, c, d) in COOP_CLASSES and not okp and not okd:
             continue
         with open(os.path.join(here, "gen", f"k_eri_{i:02d}.cu"), "w") as f:
             f.write("// Generated by quax_b200/csrc/gen_eri.py -- do not edit by hand.\n")
-            f.write(f"// ERI kernels of class ({a}{b}|{c}{d}).\n")
-            f.write('#include "../qx_kernels.cuh"\n')
-            f.write(f"QX_DEFINE_LAUNCH({i}, {a}, {b}, {c}, {d})\n")
+            f.write(f"// Kernels of class ({a}{b}|{c}{d}).\n")
+            f.write('#include "../qx_warp.cuh"\n')
+            f.write("using namespace qx;\n")
+            if (a, b, c, d) not in COOP_CLASSES:
+                f.write(f"QX_DEFINE_LAUNCH({i}, {a}, {b}, {c}, {d})\n")
+            if okp:
+                f.write(gen_warp_code(i, a, b, c, d, 0, pp) + "\n")
+            if okd:
+                f.write(gen_warp_code(i, a, b, c, d, 1, pd) + "\n")
+    with open(os.path.join(here, "gen", "warp_index.cuh"), "w") as f:
+        f.write("// Generated by quax_b200/csrc/gen_eri.py -- do not edit by hand.\n#pragma once\n")
+        f.write("#define QX_CLASS_WARP_PLAIN {" + ", ".join("1" if x else "0" for x in wp) + "}\n")
+        f.write("#define QX_CLASS_WARP_DERIV {" + ", ".join("1" if x else "0" for x in wd) + "}\n")
+        f.write("#define QX_FOR_EACH_WARP_PLAIN(X) " + " ".join(f"X({i:02d})" for i, x in enumerate(wp) if x) + "\n")
+        f.write("#define QX_FOR_EACH_WARP_DERIV(X) " + " ".join(f"X({i:02d})" for i, x in enumerate(wd) if x) + "\n")
     with open(os.path.join(here, "gen", "der_tables.cuh"), "w") as f:
         f.write(gen_coop_deriv(list(enumerate(qc))))
 

@@ -37,7 +37,60 @@ struct DerArgs {
     double cj, ck;
     double* grad;  // MODE_GRAD: 3N
     int slice;     // MODE_DER_SLICE: nuclear index
+    // split mode: accumulators were summed into acc_in[qi * nacc + t] by k_der_vrr,
+    // so k_der only runs the HRR and the epilogue
+    const double* acc_in;
 };
+
+// One task per warp: (quartet, first primitive quartet) of a fixed chunk; the warp
+// runs the VRR over the chunk into shared-memory accumulators and adds them to the
+// quartet's global accumulators.  Used for the largest classes, where one quartet's
+// primitive loop is too long for a single block to carry the class alone.
+constexpr int DER_CHUNK = 64;
+
+__global__ void __launch_bounds__(32) k_der_vrr(DerArgs da, const int2* __restrict__ tasks, long long ntask,
+                                                double* __restrict__ acc_out) {
+    const EriArgs& a = da.e;
+    const DerClass& C = da.c;
+    const int lane = threadIdx.x & 31;
+    const long long ti = blockIdx.x;
+    if (ti >= ntask) return;
+    extern __shared__ double dv_sm[];
+    double* V = dv_sm;
+    double* accw = dv_sm + C.vslots;
+    double* coef = accw + C.nacc;
+    const int2 task = tasks[ti];
+    const int2 pq = a.quartets[task.x];
+    const PairInfo P = a.pairs[pq.x];
+    const PairInfo Q = a.pairs[pq.y];
+    const uint4* __restrict__ vn = g_der_vnodes + C.vnode_off;
+    const int* __restrict__ vl = g_der_vlev + C.vlev_off;
+    const unsigned short* __restrict__ tg = g_der_targets + C.tgt_off;
+    const int e1 = C.nu, e2 = C.nu + C.na, e3 = C.nu + C.na + C.nb;
+    for (int t = lane; t < C.nacc; t += 32) accw[t] = 0.0;
+    const int nk = Q.nprim, ntot = P.nprim * nk;
+    const int tend = min(ntot, task.y + DER_CHUNK);
+    for (int t = task.y; t < tend; ++t) {
+        const int i = t / nk, j = t - i * nk;
+        const PrimPair p = a.prims[P.prim_off + i];
+        const PrimPair r = a.prims[Q.prim_off + j];
+        __syncwarp();
+        coop_prim_setup(p, r, C.S, lane, a.boys, V, coef);
+        __syncwarp();
+        for (int L = 0; L < C.nvlev; ++L) {
+            run_vrr_level(vn, vl[L], vl[L + 1], lane, 32, V, coef);
+            __syncwarp();
+        }
+        const double w2a = 2.0 * p.alpha, w2b = 2.0 * (p.zeta - p.alpha), w2c = 2.0 * r.alpha;
+        for (int t2 = lane; t2 < C.nacc; t2 += 32) {
+            const double w = t2 < e1 ? 1.0 : (t2 < e2 ? w2a : (t2 < e3 ? w2b : w2c));
+            accw[t2] = fma(w, V[tg[t2]], accw[t2]);
+        }
+    }
+    __syncwarp();
+    double* dst = acc_out + (size_t)task.x * C.nacc;
+    for (int t = lane; t < C.nacc; t += 32) atomicAdd(dst + t, accw[t]);
+}
 
 __device__ __forceinline__ void atomic_images(double* __restrict__ out, long long n, long long i, long long j,
                                               long long k, long long l, bool s12, bool s34, bool sPQ, double v) {
@@ -78,7 +131,7 @@ __global__ void __launch_bounds__(128) k_der(DerArgs da, int mode) {
     const unsigned short* __restrict__ tg = g_der_targets + C.tgt_off;
     const int e1 = C.nu, e2 = C.nu + C.na, e3 = C.nu + C.na + C.nb;
     for (int t = lane; t < C.nacc; t += 32) accw[t] = 0.0;
-    const int nk = Q.nprim, ntot = P.nprim * nk;
+    const int nk = Q.nprim, ntot = da.acc_in ? 0 : P.nprim * nk;
     for (int t = warp; t < ntot; t += W) {
         const int i = t / nk, j = t - i * nk;
         const PrimPair p = a.prims[P.prim_off + i];
@@ -101,7 +154,11 @@ __global__ void __launch_bounds__(128) k_der(DerArgs da, int mode) {
     double* acc0 = der_sm + da.region;
     for (int t = tid; t < C.nacc; t += NT) {
         double s = 0.0;
-        for (int w = 0; w < W; ++w) s += acc0[(size_t)w * C.nacc + t];
+        if (da.acc_in) {
+            s = da.acc_in[(size_t)qi * C.nacc + t];
+        } else {
+            for (int w = 0; w < W; ++w) s += acc0[(size_t)w * C.nacc + t];
+        }
         H[t] = s;
     }
     const int NB = (C.lb + 1) * (C.lb + 2) / 2, NC = (C.lc + 1) * (C.lc + 2) / 2, ND = (C.ld + 1) * (C.ld + 2) / 2;
@@ -214,6 +271,17 @@ static void der_plan(const DerClass& C, int& W, int& region, size_t& smem) {
     }
 }
 
+// HRR-only launches (split mode): four warps, no VRR buffers beyond the HRR's.
+static void der_plan_hrr(const DerClass& C, int& W, int& region, size_t& smem) {
+    W = 4;
+    region = C.hslots;
+    smem = sizeof(double) * ((size_t)region + (size_t)W * (C.nacc + 24) + C.nout);
+    if (smem > 220 * 1024) {
+        W = 1;
+        smem = sizeof(double) * ((size_t)region + (size_t)(C.nacc + 24) + C.nout);
+    }
+}
+
 size_t qx_der_smem(int der_idx) {
     int W, region;
     size_t smem;
@@ -221,12 +289,43 @@ size_t qx_der_smem(int der_idx) {
     return smem;
 }
 
+// Split mode for the largest classes: `tasks` (quartet, first primitive quartet)
+// chunks run the VRR into `scratch` (nq * nacc doubles, zeroed here), then the
+// HRR-and-epilogue kernel reads the sums.
+void qx_launch_der_split(int der_idx, const qx::EriArgs& a, int mode, const double* D, double cj, double ck,
+                         double* grad, int slice, const int2* tasks, long long ntask, double* scratch, cudaStream_t s) {
+    using namespace qx;
+    DerArgs da;
+    da.e = a;
+    da.c = g_der_classes[der_idx];
+    da.D = D;
+    da.cj = cj;
+    da.ck = ck;
+    da.grad = grad;
+    da.slice = slice;
+    da.acc_in = nullptr;
+    if (!a.nq) return;
+    cudaMemsetAsync(scratch, 0, sizeof(double) * (size_t)a.nq * da.c.nacc, s);
+    const size_t vsm = sizeof(double) * ((size_t)da.c.vslots + da.c.nacc + 24);
+    if (vsm > 48 * 1024) cudaFuncSetAttribute(k_der_vrr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vsm);
+    if (ntask) k_der_vrr<<<(unsigned)ntask, 32, vsm, s>>>(da, tasks, ntask, scratch);
+    size_t smem;
+    der_plan_hrr(da.c, da.W, da.region, smem);
+    da.acc_in = scratch;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_der, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_der<<<(unsigned)a.nq, da.W * 32, smem, s>>>(da, mode);
+}
+
+long long qx_der_nacc(int der_idx) { return g_der_classes[der_idx].nacc; }
+int qx_der_chunk() { return qx::DER_CHUNK; }
+
 void qx_launch_der(int der_idx, const qx::EriArgs& a, int mode, const double* D, double cj, double ck, double* grad,
                    int slice, cudaStream_t s) {
     using namespace qx;
     DerArgs da;
     da.e = a;
     da.c = g_der_classes[der_idx];
+    da.acc_in = nullptr;
     size_t smem;
     der_plan(da.c, da.W, da.region, smem);
     da.D = D;

@@ -18,13 +18,15 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
 #include <vector>
 
 #include "quax_b200.h"
-#include "qx_kernels.cuh"
+#include "qx_warp.cuh"
+#include "gen/warp_index.cuh"
 
 using namespace qx;
 
@@ -86,8 +88,25 @@ static const int g_class_l[QX_NUM_CLASSES][4] = {
 };
 static int g_coop_idx[QX_NUM_CLASSES];
 static int g_der_idx[QX_NUM_CLASSES];
-
+static const int g_class_nacc[QX_NUM_CLASSES] = QX_CLASS_NACC;
+static const int g_has_warp_plain[QX_NUM_CLASSES] = QX_CLASS_WARP_PLAIN;
+static const int g_has_warp_deriv[QX_NUM_CLASSES] = QX_CLASS_WARP_DERIV;
+static WarpLaunch g_warp_plain[QX_NUM_CLASSES];
+static WarpLaunch g_warp_deriv[QX_NUM_CLASSES];
+#define QX_DECL_WP(id) void qx_launch_warp_p##id(const qx::WarpArgs&, int, cudaStream_t);
+QX_FOR_EACH_WARP_PLAIN(QX_DECL_WP)
+#define QX_DECL_WD(id) void qx_launch_warp_d##id(const qx::WarpArgs&, int, cudaStream_t);
+QX_FOR_EACH_WARP_DERIV(QX_DECL_WD)
+// Engines per class.  Plain ERI: straight-line per-thread kernels (small classes),
+// warp-per-quartet kernels (lanes = primitive quartets), or the cooperative engine
+// (classes whose VRR does not fit a lane's registers).  Derivatives: warp kernels
+// where they fit, else the cooperative derivative engine.
+enum { ENG_SL = 0, ENG_WARP = 1, ENG_COOP = 2 };
 int qx_der_index(int cls);
+void qx_launch_der_split(int der_idx, const qx::EriArgs& a, int mode, const double* D, double cj, double ck,
+                         double* grad, int slice, const int2* tasks, long long ntask, double* scratch, cudaStream_t s);
+long long qx_der_nacc(int der_idx);
+int qx_der_chunk();
 void qx_launch_der(int der_idx, const qx::EriArgs& a, int mode, const double* D, double cj, double ck, double* grad,
                    int slice, cudaStream_t s);
 enum { QX_MODE_DER_DENSE = 10, QX_MODE_DER_SLICE = 11, QX_MODE_GRAD = 12 };
@@ -97,7 +116,13 @@ static bool init_class_tables() {
         g_class_scratch[c] = 0;
         g_coop_idx[c] = g_class_coop[c] ? qx_coop_index(c) : -1;
         g_der_idx[c] = qx_der_index(c);
+        g_warp_plain[c] = nullptr;
+        g_warp_deriv[c] = nullptr;
     }
+#define QX_SET_WP(id) g_warp_plain[1##id - 100] = &qx_launch_warp_p##id;
+    QX_FOR_EACH_WARP_PLAIN(QX_SET_WP)
+#define QX_SET_WD(id) g_warp_deriv[1##id - 100] = &qx_launch_warp_d##id;
+    QX_FOR_EACH_WARP_DERIV(QX_SET_WD)
 #define QX_SL_ENTRY(id, a, b, c, d)                            \
     g_eri_launch[id] = &qx_launch_eri_##id;                    \
     g_class_scratch[id] = qx::scratch_per_quartet<a, b, c, d>();
@@ -143,6 +168,11 @@ struct ClassWork {
     long long prims = 0;       // primitive quartets of the class
     int log2g = 0;             // lanes per quartet = 2^log2g
     double* scratch = nullptr; // global accumulators (ACC_GLOBAL classes), owned
+    // derivative split mode (largest classes): primitive-chunk tasks and the
+    // per-quartet accumulator sums
+    int2* d_dtasks = nullptr;
+    long long ndtask = 0;
+    double* d_dacc = nullptr;
 };
 
 static constexpr int QX_NSTREAMS = 8;
@@ -182,7 +212,40 @@ struct qx_handle {
     cudaEvent_t done[QX_NSTREAMS] = {};
     cudaEvent_t start = nullptr;
     int order[QX_NUM_CLASSES];  // classes by decreasing primitive work
+    int plain_eng[QX_NUM_CLASSES];
+    int deriv_eng[QX_NUM_CLASSES];
+    int wpq[QX_NUM_CLASSES];  // warps per quartet for the warp kernels
 };
+
+// Warps per quartet: classes with few quartets but long primitive loops let four
+// warps share a quartet so the GPU fills up.
+static int choose_wpq(long long nq, long long prims) {
+    const double avg = nq ? (double)prims / nq : 0.0;
+    return (nq < 20000 && avg >= 4 * 32) ? 4 : 1;
+}
+
+// Default engine choice, overridable with QX_PLAIN_ENGINE=sl|warp|coop and
+// QX_DERIV_ENGINE=warp|coop (for measuring alternatives); an override that a class
+// cannot honour falls back to the default.
+static void choose_engines(qx_handle* h) {
+    const char* pe = std::getenv("QX_PLAIN_ENGINE");
+    const char* de = std::getenv("QX_DERIV_ENGINE");
+    for (int c = 0; c < QX_NUM_CLASSES; ++c) {
+        int p;
+        if (g_has_warp_plain[c] && g_class_nacc[c] > 48) p = ENG_WARP;
+        else if (!g_class_coop[c]) p = ENG_SL;
+        else p = g_has_warp_plain[c] ? ENG_WARP : ENG_COOP;
+        if (pe) {
+            if (!std::strcmp(pe, "sl") && !g_class_coop[c]) p = ENG_SL;
+            if (!std::strcmp(pe, "warp") && g_has_warp_plain[c]) p = ENG_WARP;
+            if (!std::strcmp(pe, "coop") && g_class_coop[c]) p = ENG_COOP;
+        }
+        int d = g_has_warp_deriv[c] ? ENG_WARP : ENG_COOP;
+        if (de && !std::strcmp(de, "coop")) d = ENG_COOP;
+        h->plain_eng[c] = p;
+        h->deriv_eng[c] = d;
+    }
+}
 
 static int pair_index(int s1, int s2) { return s1 * (s1 + 1) / 2 + s2; }  // s1 >= s2
 
@@ -193,7 +256,12 @@ static void free_handle(qx_handle* h) {
     cudaFree(h->d_boys);
     cudaFree(h->d_err);
     cudaFree(h->d_scratch);
-    for (auto& w : h->work) { cudaFree(w.d_q); cudaFree(w.scratch); }
+    for (auto& w : h->work) {
+        cudaFree(w.d_q);
+        cudaFree(w.scratch);
+        cudaFree(w.d_dtasks);
+        cudaFree(w.d_dacc);
+    }
     for (int i = 0; i < QX_NSTREAMS; ++i) {
         if (h->streams[i]) cudaStreamDestroy(h->streams[i]);
         if (h->done[i]) cudaEventDestroy(h->done[i]);
@@ -210,6 +278,7 @@ static double dfact(int n) {
 
 static int run_class(qx_handle* h, int cls, int mode, const int2* d_q, long long nq, double* out, long long n,
                      long long base, cudaStream_t s, int log2g = 0, double* scratch = nullptr) {
+    const int eng = h->plain_eng[cls];
     EriArgs a;
     a.quartets = d_q;
     a.nq = nq;
@@ -220,10 +289,22 @@ static int run_class(qx_handle* h, int cls, int mode, const int2* d_q, long long
     a.n = n;
     a.base = base;
     a.scratch = scratch ? scratch : h->d_scratch;
-    a.log2g = g_class_coop[cls] ? 0 : log2g;
+    a.log2g = eng == ENG_SL ? log2g : 0;
     a.err = h->d_err;
-    if (g_class_coop[cls]) qx_launch_coop(g_coop_idx[cls], a, mode, s);
-    else g_eri_launch[cls](a, mode, s);
+    if (eng == ENG_COOP) {
+        qx_launch_coop(g_coop_idx[cls], a, mode, s);
+    } else if (eng == ENG_WARP) {
+        WarpArgs wa;
+        wa.e = a;
+        wa.wpq = h->wpq[cls];
+        wa.D = nullptr;
+        wa.cj = wa.ck = 0.0;
+        wa.grad = nullptr;
+        wa.slice = -1;
+        g_warp_plain[cls](wa, mode, s);
+    } else {
+        g_eri_launch[cls](a, mode, s);
+    }
     QX_CUDA(cudaGetLastError());
     return QX_OK;
 }
@@ -241,6 +322,8 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
         if (!std::isfinite(coords[i])) return fail(QX_E_INVALID, "qx_initialize: non-finite coordinate %d", i);
     qx_handle* h = new qx_handle();
     cudaGetDevice(&h->device);
+    choose_engines(h);
+    for (int c = 0; c < QX_NUM_CLASSES; ++c) h->wpq[c] = 1;
     h->natom = natom;
     h->nshell = nshell;
     h->pure = pure;
@@ -432,14 +515,28 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
         ClassWork& w = h->work[c];
         w.nq = (long long)sorted.size();
         w.prims = prims;
-        w.log2g = g_class_coop[c] ? 0 : choose_log2g(w.nq, prims);
+        w.log2g = h->plain_eng[c] == ENG_SL ? choose_log2g(w.nq, prims) : 0;
+        h->wpq[c] = choose_wpq(w.nq, prims);
         w.unique_base = base;
         base += w.nq * g_class_nout[c];
         h->nunique += w.nq;
         if (w.nq) {
             QX_ALLOC(w.d_q, sizeof(int2) * w.nq);
             cudaMemcpy(w.d_q, sorted.data(), sizeof(int2) * w.nq, cudaMemcpyHostToDevice);
-            if (g_class_scratch[c]) QX_ALLOC(w.scratch, sizeof(double) * g_class_scratch[c] * launch_threads(w.nq, w.log2g));
+            if (h->deriv_eng[c] == ENG_COOP && g_der_idx[c] >= 0) {
+                std::vector<int2> tasks;
+                const int ch = qx_der_chunk();
+                for (long long qi = 0; qi < w.nq; ++qi) {
+                    const int np_q = h->pairs[sorted[qi].x].nprim * h->pairs[sorted[qi].y].nprim;
+                    for (int t0 = 0; t0 < np_q; t0 += ch) tasks.push_back(make_int2((int)qi, t0));
+                }
+                w.ndtask = (long long)tasks.size();
+                QX_ALLOC(w.d_dtasks, sizeof(int2) * tasks.size());
+                cudaMemcpy(w.d_dtasks, tasks.data(), sizeof(int2) * tasks.size(), cudaMemcpyHostToDevice);
+                QX_ALLOC(w.d_dacc, sizeof(double) * w.nq * qx_der_nacc(g_der_idx[c]));
+            }
+            if (g_class_scratch[c] && h->plain_eng[c] == ENG_SL)
+                QX_ALLOC(w.scratch, sizeof(double) * g_class_scratch[c] * launch_threads(w.nq, w.log2g));
         }
     }
     h->unique_size = base;
@@ -582,8 +679,23 @@ static int run_all_deriv(qx_handle* h, int mode, double* out, const double* D, d
     for (int oi = 0; oi < QX_NUM_CLASSES; ++oi) {
         const int c = h->order[oi];
         if (!h->work[c].nq) continue;
-        if (g_der_idx[c] < 0) return fail(QX_E_UNSUPPORTED, "no derivative program for class %d", c);
-        qx_launch_der(g_der_idx[c], class_args(h, c, out), mode, D, cj, ck, grad, slice, h->streams[k++ % QX_NSTREAMS]);
+        cudaStream_t cs = h->streams[k++ % QX_NSTREAMS];
+        if (h->deriv_eng[c] == ENG_WARP) {
+            WarpArgs wa;
+            wa.e = class_args(h, c, out);
+            wa.wpq = h->wpq[c];
+            wa.D = D;
+            wa.cj = cj;
+            wa.ck = ck;
+            wa.grad = grad;
+            wa.slice = slice;
+            g_warp_deriv[c](wa, mode, cs);
+        } else {
+            if (g_der_idx[c] < 0) return fail(QX_E_UNSUPPORTED, "no derivative program for class %d", c);
+            const ClassWork& w = h->work[c];
+            qx_launch_der_split(g_der_idx[c], class_args(h, c, out), mode, D, cj, ck, grad, slice, w.d_dtasks,
+                                w.ndtask, w.d_dacc, cs);
+        }
         QX_CUDA(cudaGetLastError());
     }
     for (int i = 0; i < QX_NSTREAMS; ++i) {

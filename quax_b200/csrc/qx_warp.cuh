@@ -1,0 +1,273 @@
+// qx_warp.cuh -- warp-per-quartet kernels: lanes = primitive quartets.
+//
+// One warp owns one contracted shell quartet.  Its 32 lanes take 32 primitive
+// quartets at a time and each runs the class's generated straight-line VRR in
+// registers.  Every VRR target (times its weight, for the derivative sets) is an
+// "item"; items are staged 16 at a time and folded across the warp with a
+// transposing butterfly of shuffles (reduce16: 16 shuffles per 16 items per lane),
+// after which lane 2j holds the warp sum of item j and adds it to the warp's
+// shared-memory accumulator.  So no lane keeps a full accumulator set -- the
+// obstacle for straight-line per-thread code on classes with hundreds of
+// targets -- and the per-primitive work stays in registers.  After the primitive
+// loop the warp runs the class's table-driven HRR program on the accumulators
+// (lanes in parallel, level by level) and the usual epilogues.
+#pragma once
+#include "qx_kernels.cuh"
+
+namespace qx {
+
+struct WarpArgs {
+    EriArgs e;
+    int wpq;  // warps per quartet: 1 (a block holds 4 quartets) or 4 (a block holds one)
+    const double* D;  // adjoint: density (n x n)
+    double cj, ck;
+    double* grad;  // adjoint: 3N
+    int slice;     // single derivative slice
+};
+
+enum { WMODE_DENSE = 0, WMODE_UNIQUE = 1, WMODE_SCHWARZ = 2, WMODE_DER_DENSE = 10, WMODE_DER_SLICE = 11,
+       WMODE_GRAD = 12 };
+
+constexpr int WARP_QPB = 4;  // quartets (warps) per block
+
+// Sum item k of the 16 staged values over the warp; lane 2j ends with item j.
+__device__ __forceinline__ void reduce16(double (&v)[16], double* __restrict__ acc16, unsigned lane) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const bool up = lane & 16;
+        const double send = up ? v[i] : v[i + 8];
+        const double keep = up ? v[i + 8] : v[i];
+        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const bool up = lane & 8;
+        const double send = up ? v[i] : v[i + 4];
+        const double keep = up ? v[i + 4] : v[i];
+        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        const bool up = lane & 4;
+        const double send = up ? v[i] : v[i + 2];
+        const double keep = up ? v[i + 2] : v[i];
+        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+    }
+    {
+        const bool up = lane & 2;
+        const double send = up ? v[0] : v[1];
+        const double keep = up ? v[1] : v[0];
+        v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+    }
+    v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
+    if (!(lane & 1)) acc16[(lane >> 1) & 15] += v[0];
+}
+
+// Table-driven HRR level loop for one warp.  Node (uint2): x = dst | s1<<16,
+// y = s2 | side<<16 | dir<<18 ; V[dst] = V[s1] + g[side,dir] V[s2] with
+// g = AB (side 0), CD (side 1), -(dir+1) (side 2), 0 (side 3).
+template <class OnOut>
+__device__ __forceinline__ void warp_hrr(const uint2* __restrict__ hn, const int* __restrict__ hl, int nhlev,
+                                         const unsigned short* __restrict__ ho, double* H, const double* geo,
+                                         unsigned lane, OnOut&& on_out) {
+    for (int L = 0; L < nhlev; ++L) {
+        const int end = __ldg(hl + L + 1);
+        for (int nn = __ldg(hl + L) + lane; nn < end; nn += 32) {
+            const uint2 d = __ldg(hn + nn);
+            const int side = (d.y >> 16) & 3, dir = (d.y >> 18) & 3;
+            const double g = geo[side < 2 ? 3 * side + dir : (side == 2 ? 6 + dir : 10)];
+            const double v = fma(g, H[d.y & 0xffff], H[d.x >> 16]);
+            H[d.x & 0xffff] = v;
+            if (ho) {
+                const int ob = __ldg(ho + nn);
+                if (ob != 0xFFFF) on_out(ob, v);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+__device__ __forceinline__ void dense_images(double* __restrict__ out, long long n, long long i, long long j,
+                                             long long k, long long l, bool s12, bool s34, bool sPQ, double v) {
+    out[((i * n + j) * n + k) * n + l] = v;
+    if (s12) out[((j * n + i) * n + k) * n + l] = v;
+    if (s34) out[((i * n + j) * n + l) * n + k] = v;
+    if (s12 && s34) out[((j * n + i) * n + l) * n + k] = v;
+    if (sPQ) {
+        out[((k * n + l) * n + i) * n + j] = v;
+        if (s34) out[((l * n + k) * n + i) * n + j] = v;
+        if (s12) out[((k * n + l) * n + j) * n + i] = v;
+        if (s12 && s34) out[((l * n + k) * n + j) * n + i] = v;
+    }
+}
+
+__device__ __forceinline__ void atomic_images_w(double* __restrict__ out, long long n, long long i, long long j,
+                                                long long k, long long l, bool s12, bool s34, bool sPQ, double v) {
+    atomicAdd(out + ((i * n + j) * n + k) * n + l, v);
+    if (s12) atomicAdd(out + ((j * n + i) * n + k) * n + l, v);
+    if (s34) atomicAdd(out + ((i * n + j) * n + l) * n + k, v);
+    if (s12 && s34) atomicAdd(out + ((j * n + i) * n + l) * n + k, v);
+    if (sPQ) {
+        atomicAdd(out + ((k * n + l) * n + i) * n + j, v);
+        if (s34) atomicAdd(out + ((l * n + k) * n + i) * n + j, v);
+        if (s12) atomicAdd(out + ((k * n + l) * n + j) * n + i, v);
+        if (s12 && s34) atomicAdd(out + ((l * n + k) * n + j) * n + i, v);
+    }
+}
+
+// W: generated class (VRR + table offsets); DERIV selects the derivative program.
+template <class W, int DERIV>
+__global__ void __launch_bounds__(WARP_QPB * 32) k_warp(WarpArgs wa, int mode) {
+    const EriArgs& a = wa.e;
+    const unsigned lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    // wpq = 4: the block's four warps split one quartet's primitive batches
+    const int wpq = wa.wpq;
+    const int sub = warp % wpq;
+    const long long qi = (long long)blockIdx.x * (WARP_QPB / wpq) + warp / wpq;
+    if (qi >= a.nq) return;  // whole warp (whole block when wpq = 4)
+    extern __shared__ double warp_sm[];
+    double* H = warp_sm + (size_t)warp * W::SMEM_PER_WARP;  // accumulators = HRR leaves
+    double* geo = H + W::HSLOTS;                             // 11 geometry / constant factors
+    double* gam = geo + 16;                                  // adjoint: Gamma weights (NOUT)
+    const int2 pq = a.quartets[qi];
+    const PairInfo P = a.pairs[pq.x];
+    const PairInfo Q = a.pairs[pq.y];
+    const int atA = P.atom1, atB = P.atom2, atC = Q.atom1, atD = Q.atom2;
+    if (DERIV) {
+        if (atA == atB && atA == atC && atA == atD) return;  // reference skips these
+        if (mode == WMODE_DER_SLICE) {
+            const int sa = wa.slice / 3;
+            if (atA != sa && atB != sa && atC != sa && atD != sa) return;
+        }
+    }
+    for (int t = lane; t < W::NITEM_PAD; t += 32) H[t] = 0.0;
+    __syncwarp();
+    const int nk = Q.nprim, ntot = P.nprim * nk;
+    for (int t0 = 32 * sub; t0 < ntot; t0 += 32 * wpq) {
+        const int t = t0 + (int)lane;
+        const bool act = t < ntot;
+        const int tt = act ? t : 0;
+        const int i = tt / nk, j = tt - i * nk;
+        const PrimPair p = a.prims[P.prim_off + i];
+        const PrimPair r = a.prims[Q.prim_off + j];
+        PrimQ q;
+        double Fp[W::S + 1];
+        prim_setup<W::S>(p, r, a.boys, q, Fp);
+        if (!act) {
+#pragma unroll
+            for (int m = 0; m <= W::S; ++m) Fp[m] = 0.0;
+        }
+        W::vrr(Fp, q, 2.0 * p.alpha, 2.0 * (p.zeta - p.alpha), 2.0 * r.alpha, H, lane);
+        __syncwarp();
+    }
+    if (wpq > 1) {
+        // sum the four warps' accumulators into warp 0's; warp 0 finishes alone
+        __syncthreads();
+        for (int t = threadIdx.x; t < W::NITEM_PAD; t += 32 * WARP_QPB) {
+            double s = 0.0;
+#pragma unroll
+            for (int w = 1; w < WARP_QPB; ++w) s += warp_sm[(size_t)w * W::SMEM_PER_WARP + t];
+            warp_sm[t] += s;
+        }
+        __syncthreads();
+        if (warp != 0) return;
+    }
+    if (lane == 0) {
+        geo[0] = P.ABx; geo[1] = P.ABy; geo[2] = P.ABz;
+        geo[3] = Q.ABx; geo[4] = Q.ABy; geo[5] = Q.ABz;
+        geo[6] = -1.0; geo[7] = -2.0; geo[8] = -3.0; geo[9] = -4.0; geo[10] = 0.0;
+    }
+    constexpr int NB = ncart_h(W::LB), NC = ncart_h(W::LC), ND = ncart_h(W::LD);
+    const bool s12 = P.s1 != P.s2, s34 = Q.s1 != Q.s2, sPQ = pq.x != pq.y;
+    const long long n = a.n;
+    if (DERIV && mode == WMODE_GRAD) {
+        const double* __restrict__ Dm = wa.D;
+        const double fJ = (1.0 + sPQ) * (1.0 + s12) * (1.0 + s34), fK = 1.0 + sPQ;
+        const double kd = 1.0 + (double)(s12 && s34), kx = (double)s12 + (double)s34;
+        for (int o = lane; o < W::NOUT; o += 32) {
+            const int id = o % ND, ic = (o / ND) % NC, ib = (o / (ND * NC)) % NB, ia = o / (ND * NC * NB);
+            const long long ii = P.bf1 + ia, jj = P.bf2 + ib, kk = Q.bf1 + ic, ll = Q.bf2 + id;
+            gam[o] = wa.cj * fJ * __ldg(Dm + ii * n + jj) * __ldg(Dm + kk * n + ll) +
+                     wa.ck * fK * (__ldg(Dm + ii * n + kk) * __ldg(Dm + jj * n + ll) * kd +
+                                   __ldg(Dm + ii * n + ll) * __ldg(Dm + jj * n + kk) * kx);
+        }
+    }
+    __syncwarp();
+    if (!DERIV) {
+        warp_hrr(W::hnodes(), W::hlev(), W::NHLEV, nullptr, H, geo, lane, [](int, double) {});
+        const unsigned short* __restrict__ outs = W::outs();
+        if (mode == WMODE_UNIQUE) {
+            for (int o = lane; o < W::NOUT; o += 32) a.out[a.base + (long long)o * a.nq + qi] = H[__ldg(outs + o)];
+        } else if (mode == WMODE_SCHWARZ) {
+            double mx = 0.0;
+            for (int o = lane; o < W::NOUT; o += 32) {
+                const int ab = o / (NC * ND), cd = o % (NC * ND);
+                if (ab == cd) mx = fmax(mx, fabs(H[__ldg(outs + o)]));
+            }
+            for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+            if (lane == 0) a.out[pq.x] = mx;
+        } else {
+            for (int o = lane; o < W::NOUT; o += 32) {
+                const int id = o % ND, ic = (o / ND) % NC, ib = (o / (ND * NC)) % NB, ia = o / (ND * NC * NB);
+                dense_images(a.out, n, P.bf1 + ia, P.bf2 + ib, Q.bf1 + ic, Q.bf2 + id, s12, s34, sPQ, H[__ldg(outs + o)]);
+            }
+        }
+        return;
+    }
+    // derivative programs: the epilogue runs at each output node
+    double g9[9];
+#pragma unroll
+    for (int b = 0; b < 9; ++b) g9[b] = 0.0;
+    const int atoms[3] = {atA, atB, atC};
+    const long long n4 = n * n * n * n;
+    warp_hrr(W::hnodes(), W::hlev(), W::NHLEV, W::outs(), H, geo, lane, [&](int ob, double v) {
+        const int blk = ob / W::NOUT, o = ob - blk * W::NOUT;
+        if (mode == WMODE_GRAD) {
+            const double c = gam[o] * v;
+#pragma unroll
+            for (int b = 0; b < 9; ++b) g9[b] += (b == blk) ? c : 0.0;
+            return;
+        }
+        const int cen = blk / 3, xyz = blk - 3 * cen;
+        const int atc = atoms[cen];
+        if (atc == atD) return;
+        const int id = o % ND, ic = (o / ND) % NC, ib = (o / (ND * NC)) % NB, ia = o / (ND * NC * NB);
+        const long long ii = P.bf1 + ia, jj = P.bf2 + ib, kk = Q.bf1 + ic, ll = Q.bf2 + id;
+        const int sp = 3 * atc + xyz, sm = 3 * atD + xyz;
+        if (mode == WMODE_DER_DENSE) {
+            atomic_images_w(a.out + (long long)sp * n4, n, ii, jj, kk, ll, s12, s34, sPQ, v);
+            atomic_images_w(a.out + (long long)sm * n4, n, ii, jj, kk, ll, s12, s34, sPQ, -v);
+        } else {
+            if (sp == wa.slice) atomic_images_w(a.out, n, ii, jj, kk, ll, s12, s34, sPQ, v);
+            if (sm == wa.slice) atomic_images_w(a.out, n, ii, jj, kk, ll, s12, s34, sPQ, -v);
+        }
+    });
+    if (mode == WMODE_GRAD) {
+#pragma unroll
+        for (int b = 0; b < 9; ++b)
+            for (int off = 16; off > 0; off >>= 1) g9[b] += __shfl_xor_sync(0xffffffffu, g9[b], off);
+        if (lane == 0) {
+            for (int x = 0; x < 3; ++x) {
+                atomicAdd(wa.grad + 3 * atA + x, g9[x]);
+                atomicAdd(wa.grad + 3 * atB + x, g9[3 + x]);
+                atomicAdd(wa.grad + 3 * atC + x, g9[6 + x]);
+                atomicAdd(wa.grad + 3 * atD + x, -(g9[x] + g9[3 + x] + g9[6 + x]));
+            }
+        }
+    }
+}
+
+template <class W, int DERIV>
+void launch_warp(const WarpArgs& wa, int mode, cudaStream_t s) {
+    const size_t smem = sizeof(double) * (size_t)W::SMEM_PER_WARP * WARP_QPB;
+    auto k = k_warp<W, DERIV>;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const int qpb = WARP_QPB / wa.wpq;
+    const long long nb = (wa.e.nq + qpb - 1) / qpb;
+    if (nb) k<<<(unsigned)nb, WARP_QPB * 32, smem, s>>>(wa, mode);
+}
+
+typedef void (*WarpLaunch)(const WarpArgs&, int mode, cudaStream_t);
+
+}  // namespace qx

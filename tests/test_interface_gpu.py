@@ -83,7 +83,7 @@ def test_adjoint_autograd_against_finite_differences():
             c = mol.coords.copy()
             c.flat[nu] += s * h
             e2 = EriEngine(b.with_coords(c), 1e-14)
-            Es.append(float(two_electron_energy(geom, D, e2)))
+            Es.append(float(two_electron_energy(geom.detach(), D, e2)))
             e2.close()
         fd[nu] = (Es[0] - Es[1]) / (2 * h)
     assert np.abs(g.cpu().numpy() - fd).max() < 1e-6 * max(1.0, np.abs(fd).max())
