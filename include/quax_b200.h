@@ -120,6 +120,14 @@ int qx_compute_2e_deriv(qx_handle *h, const int *deriv_vec, int len, double *out
 int qx_grad_adjoint(qx_handle *h, const double *D, double cj, double ck, double *grad, int on_device,
                     void *stream);
 
+/* Direct Coulomb and exchange matrices, replacing the dense jk_build contractions
+ * of quax/methods/hartree_fock.py:26-28,79-80,92-93 (J = jk_build(G, D),
+ * K = jk_build(G.transpose(0,2,1,3), D)) without forming G:
+ *     J_ij = sum_kl (ij|kl) D_kl,   K_ij = sum_kl (ik|jl) D_kl      (n x n, row-major)
+ * over the screened unique quartets.  J and K are overwritten; D, J, K are device
+ * pointers when on_device = 1, host pointers otherwise. */
+int qx_jk(qx_handle *h, const double *D, double *J, double *K, int on_device, void *stream);
+
 /* Angular-momentum classes (canonical (la lb|lc ld), la>=lb, lc>=ld, bra class >=
  * ket class) and per-class work of a handle: screened unique quartets, primitive
  * quartets, and algorithmic FP64 FLOPs of the plain and first-derivative programs

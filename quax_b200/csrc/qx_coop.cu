@@ -127,6 +127,13 @@ __global__ void __launch_bounds__(COOP_WPB * 32) k_coop(CoopArgs ca, int mode) {
             for (int w = 1; w < COOP_WPB; ++w) m = fmax(m, acc0[w]);
             a.out[pq.x] = m;
         }
+    } else if (mode == MODE_JK) {
+        const bool s12 = P.s1 != P.s2, s34 = Q.s1 != Q.s2, sPQ = pq.x != pq.y;
+        for (int o = tid; o < C.nout; o += NT) {
+            const int id = o % ND, ic = (o / ND) % NC, ib = (o / (ND * NC)) % NB, ia = o / (ND * NC * NB);
+            jk_images(a.out, a.out2, a.dens, a.n, P.bf1 + ia, P.bf2 + ib, Q.bf1 + ic, Q.bf2 + id, s12, s34, sPQ,
+                      H[outs[o]]);
+        }
     } else {
         const long long n = a.n;
         const bool s12 = P.s1 != P.s2, s34 = Q.s1 != Q.s2, sPQ = pq.x != pq.y;

@@ -132,7 +132,7 @@ static bool init_class_tables() {
 static const bool g_tables_ready = init_class_tables();
 
 // ------------------------------------------------------------------ Boys table --
-static void boys_table_host(std::vector<double>& tab) {
+static void boys_table_compute(std::vector<double>& tab) {
     tab.assign((size_t)BOYS_NG * BOYS_NM, 0.0);
     for (int g = 0; g < BOYS_NG; ++g) {
         const double T = g / BOYS_INV_H;
@@ -158,6 +158,14 @@ static void boys_table_host(std::vector<double>& tab) {
         }
         for (int m = 0; m < BOYS_NM; ++m) tab[(size_t)g * BOYS_NM + m] = F[m];
     }
+}
+
+// The table depends on nothing but the grid: build it once per process.
+static void boys_table_host(std::vector<double>& tab) {
+    static std::once_flag once;
+    static std::vector<double> cached;
+    std::call_once(once, [] { boys_table_compute(cached); });
+    tab = cached;
 }
 
 // ------------------------------------------------------------------ handle ----
@@ -215,7 +223,30 @@ struct qx_handle {
     int plain_eng[QX_NUM_CLASSES];
     int deriv_eng[QX_NUM_CLASSES];
     int wpq[QX_NUM_CLASSES];  // warps per quartet for the warp kernels
+    std::vector<int2> lists_host[QX_NUM_CLASSES];  // kept for lazily built derivative tasks
 };
+
+// Primitive-chunk tasks and accumulator sums of the derivative split mode, built
+// at the first derivative call that needs them.
+static int ensure_deriv_tasks(qx_handle* h, int c) {
+    ClassWork& w = h->work[c];
+    if (w.d_dtasks || !w.nq) return QX_OK;
+    const auto& L = h->lists_host[c];
+    std::vector<int2> tasks;
+    const int ch = qx_der_chunk();
+    for (size_t qi = 0; qi < L.size(); ++qi) {
+        const int np_q = h->pairs[L[qi].x].nprim * h->pairs[L[qi].y].nprim;
+        for (int t0 = 0; t0 < np_q; t0 += ch) tasks.push_back(make_int2((int)qi, t0));
+    }
+    if (cudaMalloc((void**)&w.d_dtasks, sizeof(int2) * tasks.size()) != cudaSuccess ||
+        cudaMalloc((void**)&w.d_dacc, sizeof(double) * w.nq * qx_der_nacc(g_der_idx[c])) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(QX_E_NOMEM, "derivative split-mode buffers for class %d", c);
+    }
+    w.ndtask = (long long)tasks.size();
+    QX_CUDA(cudaMemcpy(w.d_dtasks, tasks.data(), sizeof(int2) * tasks.size(), cudaMemcpyHostToDevice));
+    return QX_OK;
+}
 
 // Warps per quartet: classes with few quartets but long primitive loops let four
 // warps share a quartet so the GPU fills up.
@@ -277,7 +308,8 @@ static double dfact(int n) {
 }
 
 static int run_class(qx_handle* h, int cls, int mode, const int2* d_q, long long nq, double* out, long long n,
-                     long long base, cudaStream_t s, int log2g = 0, double* scratch = nullptr) {
+                     long long base, cudaStream_t s, int log2g = 0, double* scratch = nullptr, double* out2 = nullptr,
+                     const double* dens = nullptr) {
     const int eng = h->plain_eng[cls];
     EriArgs a;
     a.quartets = d_q;
@@ -289,6 +321,8 @@ static int run_class(qx_handle* h, int cls, int mode, const int2* d_q, long long
     a.n = n;
     a.base = base;
     a.scratch = scratch ? scratch : h->d_scratch;
+    a.out2 = out2;
+    a.dens = dens;
     a.log2g = eng == ENG_SL ? log2g : 0;
     a.err = h->d_err;
     if (eng == ENG_COOP) {
@@ -523,18 +557,7 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
         if (w.nq) {
             QX_ALLOC(w.d_q, sizeof(int2) * w.nq);
             cudaMemcpy(w.d_q, sorted.data(), sizeof(int2) * w.nq, cudaMemcpyHostToDevice);
-            if (h->deriv_eng[c] == ENG_COOP && g_der_idx[c] >= 0) {
-                std::vector<int2> tasks;
-                const int ch = qx_der_chunk();
-                for (long long qi = 0; qi < w.nq; ++qi) {
-                    const int np_q = h->pairs[sorted[qi].x].nprim * h->pairs[sorted[qi].y].nprim;
-                    for (int t0 = 0; t0 < np_q; t0 += ch) tasks.push_back(make_int2((int)qi, t0));
-                }
-                w.ndtask = (long long)tasks.size();
-                QX_ALLOC(w.d_dtasks, sizeof(int2) * tasks.size());
-                cudaMemcpy(w.d_dtasks, tasks.data(), sizeof(int2) * tasks.size(), cudaMemcpyHostToDevice);
-                QX_ALLOC(w.d_dacc, sizeof(double) * w.nq * qx_der_nacc(g_der_idx[c]));
-            }
+            if (h->deriv_eng[c] == ENG_COOP) h->lists_host[c] = sorted;  // tasks built on first use
             if (g_class_scratch[c] && h->plain_eng[c] == ENG_SL)
                 QX_ALLOC(w.scratch, sizeof(double) * g_class_scratch[c] * launch_threads(w.nq, w.log2g));
         }
@@ -597,7 +620,8 @@ static int check_err_word(qx_handle* h, cudaStream_t s) {
 
 // Launch every class on the handle's internal streams (largest work first,
 // round-robin), ordered after the caller's stream and joined back into it.
-static int run_all_classes(qx_handle* h, int mode, double* out, long long n, cudaStream_t s) {
+static int run_all_classes(qx_handle* h, int mode, double* out, long long n, cudaStream_t s, double* out2 = nullptr,
+                           const double* dens = nullptr) {
     QX_CUDA(cudaEventRecord(h->start, s));
     for (int i = 0; i < QX_NSTREAMS; ++i) QX_CUDA(cudaStreamWaitEvent(h->streams[i], h->start, 0));
     int k = 0;
@@ -606,7 +630,7 @@ static int run_all_classes(qx_handle* h, int mode, double* out, long long n, cud
         const ClassWork& w = h->work[c];
         if (!w.nq) continue;
         cudaStream_t cs = h->streams[k++ % QX_NSTREAMS];
-        int rc = run_class(h, c, mode, w.d_q, w.nq, out, n, w.unique_base, cs, w.log2g, w.scratch);
+        int rc = run_class(h, c, mode, w.d_q, w.nq, out, n, w.unique_base, cs, w.log2g, w.scratch, out2, dens);
         if (rc) return rc;
     }
     for (int i = 0; i < QX_NSTREAMS; ++i) {
@@ -666,6 +690,8 @@ static EriArgs class_args(qx_handle* h, int c, double* out) {
     a.scratch = nullptr;
     a.log2g = 0;
     a.err = h->d_err;
+    a.out2 = nullptr;
+    a.dens = nullptr;
     return a;
 }
 
@@ -692,6 +718,8 @@ static int run_all_deriv(qx_handle* h, int mode, double* out, const double* D, d
             g_warp_deriv[c](wa, mode, cs);
         } else {
             if (g_der_idx[c] < 0) return fail(QX_E_UNSUPPORTED, "no derivative program for class %d", c);
+            int rc = ensure_deriv_tasks(h, c);
+            if (rc) return rc;
             const ClassWork& w = h->work[c];
             qx_launch_der_split(g_der_idx[c], class_args(h, c, out), mode, D, cj, ck, grad, slice, w.d_dtasks,
                                 w.ndtask, w.d_dacc, cs);
@@ -819,4 +847,37 @@ extern "C" int qx_eri_unique_class(qx_handle* h, int cls, double* out_dev, void*
     if (!w.nq) return QX_OK;
     return run_class(h, cls, MODE_UNIQUE, w.d_q, w.nq, out_dev, 0, w.unique_base, (cudaStream_t)stream, w.log2g,
                      w.scratch);
+}
+
+// ---------------------------------------------------------------- direct J/K ---
+extern "C" int qx_jk(qx_handle* h, const double* D, double* J, double* K, int on_device, void* stream) {
+    if (!h || !D || !J || !K) return fail(QX_E_INVALID, "qx_jk: NULL argument");
+    DeviceGuard g(h->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const long long n = h->nbf;
+    const size_t bytes = sizeof(double) * n * n;
+    if (on_device) {
+        QX_CUDA(cudaMemsetAsync(J, 0, bytes, s));
+        QX_CUDA(cudaMemsetAsync(K, 0, bytes, s));
+        return run_all_classes(h, MODE_JK, J, n, s, K, D);
+    }
+    double* d = nullptr;
+    if (cudaMalloc((void**)&d, 3 * bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(QX_E_NOMEM, "qx_jk: staging allocation failed");
+    }
+    int rc = QX_OK;
+    cudaError_t e = cudaMemcpyAsync(d, D, bytes, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d + n * n, 0, 2 * bytes, s);
+    if (e != cudaSuccess) rc = fail(QX_E_CUDA, "qx_jk: %s", cudaGetErrorString(e));
+    if (!rc) rc = run_all_classes(h, MODE_JK, d + n * n, n, s, d + 2 * n * n, d);
+    if (!rc) {
+        e = cudaMemcpyAsync(J, d + n * n, bytes, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(K, d + 2 * n * n, bytes, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) rc = fail(QX_E_CUDA, "qx_jk: %s", cudaGetErrorString(e));
+    }
+    cudaFree(d);
+    if (!rc) rc = check_err_word(h, s);
+    return rc;
 }

@@ -9,7 +9,7 @@ namespace qx {
 __host__ __device__ constexpr int ncart_h(int l) { return (l + 1) * (l + 2) / 2; }
 
 // ------------------------------------------------------------------ kernels ---
-enum { MODE_DENSE = 0, MODE_UNIQUE = 1, MODE_SCHWARZ = 2 };
+enum { MODE_DENSE = 0, MODE_UNIQUE = 1, MODE_SCHWARZ = 2, MODE_JK = 3 };
 
 struct EriArgs {
     const int2* quartets;
@@ -21,6 +21,8 @@ struct EriArgs {
     long long n;     // MODE_DENSE: number of basis functions
     long long base;  // MODE_UNIQUE: offset of this class block
     double* scratch; // ACC_GLOBAL classes: nq * group * NACC doubles
+    double* out2;       // MODE_JK: K (out holds J)
+    const double* dens; // MODE_JK: D
     int log2g;       // log2 of the lanes cooperating on one quartet (0..5)
     int* err;
 };
@@ -46,6 +48,45 @@ struct AccPolicy {
     static constexpr int kind = NACC <= 48 ? ACC_REG : (NACC <= 220 ? ACC_SMEM : ACC_GLOBAL);
     static constexpr int bs = 128;
     static constexpr int smem = kind == ACC_SMEM ? NACC * bs * 8 : 0;
+};
+
+// Direct Coulomb/exchange build: every distinct image (p q|r s) of a unique element
+// adds v D_rs to J_pq and v D_qs to K_pr (J_ij = sum_kl (ij|kl) D_kl and
+// K_ij = sum_kl (ik|jl) D_kl, the reference's jk_build on G and on G.transpose(0,2,1,3)).
+__device__ __forceinline__ void jk_image(double* __restrict__ J, double* __restrict__ K,
+                                         const double* __restrict__ D, long long n, long long p, long long q,
+                                         long long r, long long s, double v) {
+    atomicAdd(J + p * n + q, v * __ldg(D + r * n + s));
+    atomicAdd(K + p * n + r, v * __ldg(D + q * n + s));
+}
+
+__device__ __forceinline__ void jk_images(double* __restrict__ J, double* __restrict__ K, const double* __restrict__ D,
+                                          long long n, long long i, long long j, long long k, long long l, bool s12,
+                                          bool s34, bool sPQ, double v) {
+    jk_image(J, K, D, n, i, j, k, l, v);
+    if (s12) jk_image(J, K, D, n, j, i, k, l, v);
+    if (s34) jk_image(J, K, D, n, i, j, l, k, v);
+    if (s12 && s34) jk_image(J, K, D, n, j, i, l, k, v);
+    if (sPQ) {
+        jk_image(J, K, D, n, k, l, i, j, v);
+        if (s34) jk_image(J, K, D, n, l, k, i, j, v);
+        if (s12) jk_image(J, K, D, n, k, l, j, i, v);
+        if (s12 && s34) jk_image(J, K, D, n, l, k, j, i, v);
+    }
+}
+
+template <int NA, int NB, int NC, int ND>
+struct JKStore {
+    double* __restrict__ J;
+    double* __restrict__ K;
+    const double* __restrict__ D;
+    long long n;
+    int bf1, bf2, bf3, bf4;
+    bool s12, s34, sPQ;
+    __device__ __forceinline__ void operator()(int k, double v) {
+        const int id = k % ND, ic = (k / ND) % NC, ib = (k / (ND * NC)) % NB, ia = k / (ND * NC * NB);
+        jk_images(J, K, D, n, bf1 + ia, bf2 + ib, bf3 + ic, bf4 + id, s12, s34, sPQ, v);
+    }
 };
 
 template <int NA, int NB, int NC, int ND>
@@ -129,6 +170,10 @@ __device__ __noinline__ void finish_quartet(const EriArgs& a, const PairInfo& P,
         SchwarzStore<NA, NB, NC, ND> st;
         C::hrr(acc, st, P.ABx, P.ABy, P.ABz, Q.ABx, Q.ABy, Q.ABz);
         a.out[pq.x] = st.mx;
+    } else if constexpr (MODE == MODE_JK) {
+        JKStore<NA, NB, NC, ND> st{a.out, a.out2, a.dens, a.n, P.bf1, P.bf2, Q.bf1, Q.bf2,
+                                   P.s1 != P.s2, Q.s1 != Q.s2, pq.x != pq.y};
+        C::hrr(acc, st, P.ABx, P.ABy, P.ABz, Q.ABx, Q.ABy, Q.ABz);
     } else {
         DenseStore<NA, NB, NC, ND> st{a.out, a.n, P.bf1, P.bf2, Q.bf1, Q.bf2, P.s1 != P.s2, Q.s1 != Q.s2, pq.x != pq.y};
         C::hrr(acc, st, P.ABx, P.ABy, P.ABz, Q.ABx, Q.ABy, Q.ABz);
@@ -176,6 +221,10 @@ void launch_eri(const EriArgs& a, int mode, cudaStream_t s) {
         k<<<(unsigned)nb, bs, Pol::smem, s>>>(a);
     } else if (mode == MODE_UNIQUE) {
         auto k = k_eri<LA, LB, LC, LD, MODE_UNIQUE>;
+        if (Pol::smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, Pol::smem);
+        k<<<(unsigned)nb, bs, Pol::smem, s>>>(a);
+    } else if (mode == MODE_JK) {
+        auto k = k_eri<LA, LB, LC, LD, MODE_JK>;
         if (Pol::smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, Pol::smem);
         k<<<(unsigned)nb, bs, Pol::smem, s>>>(a);
     } else if constexpr (LA == LC && LB == LD) {

@@ -207,6 +207,12 @@ __global__ void __launch_bounds__(WARP_QPB * 32) k_warp(WarpArgs wa, int mode) {
             }
             for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
             if (lane == 0) a.out[pq.x] = mx;
+        } else if (mode == MODE_JK) {
+            for (int o = lane; o < W::NOUT; o += 32) {
+                const int id = o % ND, ic = (o / ND) % NC, ib = (o / (ND * NC)) % NB, ia = o / (ND * NC * NB);
+                jk_images(a.out, a.out2, a.dens, n, P.bf1 + ia, P.bf2 + ib, Q.bf1 + ic, Q.bf2 + id, s12, s34, sPQ,
+                          H[__ldg(outs + o)]);
+            }
         } else {
             for (int o = lane; o < W::NOUT; o += 32) {
                 const int id = o % ND, ic = (o / ND) % NC, ib = (o / (ND * NC)) % NB, ia = o / (ND * NC * NB);

@@ -45,6 +45,7 @@ SIGNATURES = {
     "qx_eri_deriv_core": (C.c_int, [_vp, C.c_int, _vp, C.c_int, _vp]),
     "qx_compute_2e_deriv": (C.c_int, [_vp, _ip, C.c_int, _vp, C.c_int, _vp]),
     "qx_grad_adjoint": (C.c_int, [_vp, _vp, C.c_double, C.c_double, _vp, C.c_int, _vp]),
+    "qx_jk": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, _vp]),
     "qx_num_classes": (C.c_int, []),
     "qx_class_info": (
         C.c_int,

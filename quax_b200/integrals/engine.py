@@ -182,3 +182,20 @@ class EriEngine:
                 "qx_grad_adjoint",
             )
         return out
+
+    # -- Fock-matrix pieces -----------------------------------------------------
+    def jk(self, D: torch.Tensor, J: torch.Tensor | None = None, K: torch.Tensor | None = None, stream=None):
+        """Direct J_ij = sum (ij|kl) D_kl and K_ij = sum (ik|jl) D_kl (D symmetric)."""
+        D = D.to(device=self.device, dtype=torch.float64).contiguous()
+        n = self.nbf
+        if J is None:
+            J = torch.empty((n, n), dtype=torch.float64, device=self.device)
+        if K is None:
+            K = torch.empty((n, n), dtype=torch.float64, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.check(
+                _lib.load().qx_jk(self.handle, C.c_void_p(D.data_ptr()), C.c_void_p(J.data_ptr()),
+                                  C.c_void_p(K.data_ptr()), 1, C.c_void_p(_stream_ptr(stream))),
+                "qx_jk",
+            )
+        return J, K
