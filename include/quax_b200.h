@@ -98,14 +98,18 @@ int qx_compute_2e_int(qx_handle *h, double *out, int out_on_device, void *stream
 int qx_eri_unique(qx_handle *h, double *out_dev, void *stream);
 
 /* Replaces eri_deriv_core(order) (libint_interface.cc:2582-2779): the full
- * first-derivative tensor, 3*natom*n^4 doubles in the layout (3N, n, n, n, n),
- * nuclear index 3*atom + xyz.  Quartets whose four shells sit on one atom are
- * skipped (zero), as in the reference.  order must be 1 in this build. */
+ * derivative tensor of order 1 or 2.  Order 1: 3N*n^4 doubles, layout
+ * (3N, n, n, n, n), nuclear index 3*atom + xyz.  Order 2: M(M+1)/2 * n^4 doubles
+ * (M = 3N), one slice per nuclear pair nu1 <= nu2 in the reference's
+ * combinations-with-repetition order (utils.h:158-172, rank = nu1*M -
+ * nu1(nu1-1)/2 + nu2 - nu1).  Quartets whose four shells sit on one atom are
+ * skipped (zero), as in the reference.  Order 2 needs s and p shells only
+ * (QX_E_UNSUPPORTED otherwise). */
 int qx_eri_deriv_core(qx_handle *h, int order, double *out, int out_on_device, void *stream);
 
 /* Replaces compute_2e_deriv("eri", 0., deriv_vec) (libint_interface.cc:1097-1335):
  * one n^4 derivative slice selected by deriv_vec[3*natom] (non-negative counts;
- * total order must be 1 in this build). */
+ * total order 1 or 2, order 2 for s and p shells only). */
 int qx_compute_2e_deriv(qx_handle *h, const int *deriv_vec, int len, double *out, int out_on_device,
                         void *stream);
 

@@ -59,6 +59,8 @@ def lib():
                                         _dp, C.c_int]
         L.qxo_count_unique.restype = C.c_long
         L.qxo_count_unique.argtypes = [C.POINTER(_Basis), C.c_double, C.c_int]
+        L.qxo_shell_quartet_deriv2.argtypes = [C.POINTER(_Basis), C.c_int, C.c_int, C.c_int, C.c_int, _dp]
+        L.qxo_eri_deriv2.argtypes = [C.POINTER(_Basis), C.c_double, C.c_int, _dp, C.c_int]
         L.qxo_how_many_derivs.argtypes = [C.c_int, C.c_int]
         L.qxo_multi_index_lookup.argtypes = [C.c_int, C.c_int, _ip]
         _LIB = L
@@ -149,6 +151,24 @@ def eri_deriv1(ob: OracleBasis, thr: float, deriv_idx: int = -1, nthreads: int =
     shape = (n, n, n, n) if deriv_idx >= 0 else (3 * ob.natom, n, n, n, n)
     out = np.empty(shape)
     lib().qxo_eri_deriv1(ob.ref, thr, int(deriv_idx), _p(out), nthreads)
+    return out
+
+
+def shell_quartet_deriv2(ob: OracleBasis, s1, s2, s3, s4) -> np.ndarray:
+    """(12, 12, n1, n2, n3, n4) second-derivative blocks, index 3*centre + xyz."""
+    n = [(int(ob.l[s]) + 1) * (int(ob.l[s]) + 2) // 2 for s in (s1, s2, s3, s4)]
+    out = np.empty((12, 12) + tuple(n))
+    lib().qxo_shell_quartet_deriv2(ob.ref, s1, s2, s3, s4, _p(out))
+    return out
+
+
+def eri_deriv2(ob: OracleBasis, thr: float, pair_idx: int = -1, nthreads: int = 0) -> np.ndarray:
+    """Second-derivative tensor (3N(3N+1)/2, n, n, n, n), reference semantics."""
+    n = ob.nbf
+    N3 = 3 * ob.natom
+    shape = (n, n, n, n) if pair_idx >= 0 else (N3 * (N3 + 1) // 2, n, n, n, n)
+    out = np.empty(shape)
+    lib().qxo_eri_deriv2(ob.ref, thr, int(pair_idx), _p(out), nthreads)
     return out
 
 

@@ -758,6 +758,243 @@ long qxo_count_unique(const qxo_basis *B, double thr, int nthreads) {
     return c;
 }
 
+
+/* (a b|c d) block of a weighted set for AMs shifted by (da, db, dc) (d unchanged),
+ * cached in *slot. */
+static double *blk2(const qxo_basis *B, const int *L, const double *AB, const double *CD, const double *X, int NF,
+                    double *cached, double **slot, int da, int db, int dc) {
+    (void)B;
+    if (cached) return cached;
+    int la = L[0] + da, lb = L[1] + db, lc = L[2] + dc, ld = L[3];
+    size_t sz = (size_t)ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
+    double *o = (double *)malloc(sizeof(double) * sz);
+    hrr_both(la, lb, lc, ld, AB, CD, X, NF, o);
+    *slot = o;
+    return o;
+}
+
+/* ------------------------------------------------------- second derivatives --- */
+/* ------------------------------------------------------- second derivatives --- */
+/* Full 12 x 12 block set of second derivatives of the Cartesian quartet block
+ * (s1 s2|s3 s4): out[(P*12 + Q) * nblk + o], P, Q = 3*centre + xyz.  Applies
+ * d/dA_i g_a = 2 alpha g_{a+1_i} - a_i g_{a-1_i} twice (same-centre and cross-centre
+ * terms from ten weighted primitive sums), and the D-centre rows by translational
+ * invariance. */
+static int quartet2(const qxo_basis *B, int s1, int s2, int s3, int s4, double *out) {
+    int L[4] = {B->l[s1], B->l[s2], B->l[s3], B->l[s4]};
+    int sh[4] = {s1, s2, s3, s4};
+    const double *Cn[4];
+    for (int c = 0; c < 4; ++c) Cn[c] = B->center + 3 * sh[c];
+    double AB[3], CD[3];
+    for (int i = 0; i < 3; ++i) { AB[i] = Cn[0][i] - Cn[1][i]; CD[i] = Cn[2][i] - Cn[3][i]; }
+    double AB2 = AB[0] * AB[0] + AB[1] * AB[1] + AB[2] * AB[2];
+    double CD2 = CD[0] * CD[0] + CD[1] * CD[1] + CD[2] * CD[2];
+    int E = L[0] + L[1] + 2, F = L[2] + L[3] + 2;
+    int NE = hoff(E + 1), NF = hoff(F + 1), M = E + F + 1;
+    size_t vsz = (size_t)NE * NF * M, asz = (size_t)NE * NF;
+    /* sets: 0 U, 1 A, 2 B, 3 C, 4 AA, 5 BB, 6 CC, 7 AB, 8 AC, 9 BC */
+    double *v = (double *)malloc(sizeof(double) * (vsz + 10 * asz));
+    double *S = v + vsz;
+    memset(S, 0, sizeof(double) * 10 * asz);
+    double Fm[4 * QXO_LMAX + 8];
+    const double pref0 = 2.0 * pow(M_PI, 2.5);
+    for (int p1 = 0; p1 < B->nprim[s1]; ++p1)
+        for (int p2 = 0; p2 < B->nprim[s2]; ++p2) {
+            double a = B->alpha[B->prim_off[s1] + p1], b = B->alpha[B->prim_off[s2] + p2];
+            double zeta = a + b, P[3], PA[3];
+            for (int i = 0; i < 3; ++i) { P[i] = (a * Cn[0][i] + b * Cn[1][i]) / zeta; PA[i] = P[i] - Cn[0][i]; }
+            double Kab = exp(-a * b / zeta * AB2) * B->coef[B->prim_off[s1] + p1] * B->coef[B->prim_off[s2] + p2];
+            for (int p3 = 0; p3 < B->nprim[s3]; ++p3)
+                for (int p4 = 0; p4 < B->nprim[s4]; ++p4) {
+                    double c = B->alpha[B->prim_off[s3] + p3], d = B->alpha[B->prim_off[s4] + p4];
+                    double eta = c + d, Q[3], QC[3], W[3], WP[3], WQ[3], PQ2 = 0.0;
+                    for (int i = 0; i < 3; ++i) { Q[i] = (c * Cn[2][i] + d * Cn[3][i]) / eta; QC[i] = Q[i] - Cn[2][i]; }
+                    double Kcd = exp(-c * d / eta * CD2) * B->coef[B->prim_off[s3] + p3] * B->coef[B->prim_off[s4] + p4];
+                    double rho = zeta * eta / (zeta + eta);
+                    for (int i = 0; i < 3; ++i) {
+                        W[i] = (zeta * P[i] + eta * Q[i]) / (zeta + eta);
+                        WP[i] = W[i] - P[i];
+                        WQ[i] = W[i] - Q[i];
+                        PQ2 += (P[i] - Q[i]) * (P[i] - Q[i]);
+                    }
+                    qxo_boys(E + F, rho * PQ2, Fm);
+                    vrr(E, F, zeta, eta, PA, WP, QC, WQ, rho, Fm, pref0 / (zeta * eta * sqrt(zeta + eta)) * Kab * Kcd, v);
+                    double w2[10] = {1.0, 2 * a, 2 * b, 2 * c, 4 * a * a, 4 * b * b, 4 * c * c, 4 * a * b, 4 * a * c, 4 * b * c};
+                    for (size_t h = 0; h < (size_t)NE; ++h)
+                        for (int g = 0; g < NF; ++g) {
+                            double x = v[(h * NF + g) * M];
+                            for (int k = 0; k < 10; ++k) S[k * asz + h * NF + g] += w2[k] * x;
+                        }
+                }
+        }
+    int n[4];
+    for (int c = 0; c < 4; ++c) n[c] = ncart(L[c]);
+    size_t nblk = (size_t)n[0] * n[1] * n[2] * n[3];
+    /* shifted blocks: cache by (set, dla, dlb, dlc) with shifts in {-2..2} */
+    double *cache[10][5][5][5];
+    memset(cache, 0, sizeof cache);
+#define BLK(set, da, db, dc) blk2(B, L, AB, CD, S + (set) * asz, NF, cache[set][(da) + 2][(db) + 2][(dc) + 2], &cache[set][(da) + 2][(db) + 2][(dc) + 2], da, db, dc)
+    for (int P1 = 0; P1 < 9; ++P1)
+        for (int Q1 = 0; Q1 < 9; ++Q1) {
+            int X = P1 / 3, i = P1 % 3, Y = Q1 / 3, j = Q1 % 3;
+            double *dst = out + ((size_t)P1 * 12 + Q1) * nblk;
+            for (int ia = 0; ia < n[0]; ++ia)
+                for (int ib = 0; ib < n[1]; ++ib)
+                    for (int ic = 0; ic < n[2]; ++ic)
+                        for (int id = 0; id < n[3]; ++id) {
+                            const int *xs[4] = {g_comp[L[0]][ia], g_comp[L[1]][ib], g_comp[L[2]][ic], g_comp[L[3]][id]};
+                            int comp[4][3];
+                            for (int cc = 0; cc < 4; ++cc)
+                                for (int k = 0; k < 3; ++k) comp[cc][k] = xs[cc][k];
+                            double val = 0.0;
+                            /* enumerate the two derivative factors: each is (+1, weight set, shift +1)
+                             * or (-n, unweighted, shift -1) on its centre */
+                            for (int fx = 0; fx < 2; ++fx)
+                                for (int fy = 0; fy < 2; ++fy) {
+                                    int cm[4][3];
+                                    memcpy(cm, comp, sizeof cm);
+                                    double coef = 1.0;
+                                    if (fx == 0) cm[X][i] += 1;
+                                    else { coef *= -cm[X][i]; cm[X][i] -= 1; }
+                                    if (coef == 0.0) continue;
+                                    if (fy == 0) cm[Y][j] += 1;
+                                    else { coef *= -cm[Y][j]; cm[Y][j] -= 1; }
+                                    if (coef == 0.0) continue;
+                                    int neg = 0;
+                                    for (int cc = 0; cc < 4; ++cc)
+                                        for (int k = 0; k < 3; ++k)
+                                            if (cm[cc][k] < 0) neg = 1;
+                                    if (neg) continue;
+                                    /* weight set: product of the factors' weights */
+                                    int wX = fx == 0 ? X + 1 : 0, wY = fy == 0 ? Y + 1 : 0; /* 1 A, 2 B, 3 C */
+                                    int set;
+                                    if (!wX && !wY) set = 0;
+                                    else if (!wX || !wY) set = wX ? wX : wY;
+                                    else {
+                                        int u = wX < wY ? wX : wY, w = wX < wY ? wY : wX;
+                                        set = (u == w) ? 3 + u : (u == 1 ? (w == 2 ? 7 : 8) : 9);
+                                    }
+                                    int dl[4];
+                                    for (int cc = 0; cc < 4; ++cc) dl[cc] = cm[cc][0] + cm[cc][1] + cm[cc][2] - L[cc];
+                                    double *bk = BLK(set, dl[0], dl[1], dl[2]);
+                                    int nb2 = ncart(L[1] + dl[1]), nc2 = ncart(L[2] + dl[2]);
+                                    size_t o = (((size_t)lidx(cm[0][0], cm[0][1], cm[0][2]) * nb2 + lidx(cm[1][0], cm[1][1], cm[1][2])) * nc2 +
+                                                lidx(cm[2][0], cm[2][1], cm[2][2])) * n[3] + lidx(cm[3][0], cm[3][1], cm[3][2]);
+                                    val += coef * bk[o];
+                                }
+                            dst[(((size_t)ia * n[1] + ib) * n[2] + ic) * n[3] + id] = val;
+                        }
+        }
+    /* D rows and columns by translational invariance */
+    for (int i = 0; i < 3; ++i)
+        for (int Q1 = 0; Q1 < 9; ++Q1) {
+            double *dD = out + ((size_t)(9 + i) * 12 + Q1) * nblk, *dT = out + ((size_t)Q1 * 12 + 9 + i) * nblk;
+            for (size_t o = 0; o < nblk; ++o) {
+                double s = 0.0;
+                for (int X = 0; X < 3; ++X) s += out[((size_t)(3 * X + i) * 12 + Q1) * nblk + o];
+                dD[o] = -s;
+                dT[o] = -s;
+            }
+        }
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            double *dst = out + ((size_t)(9 + i) * 12 + 9 + j) * nblk;
+            for (size_t o = 0; o < nblk; ++o) {
+                double s = 0.0;
+                for (int X = 0; X < 3; ++X) s += out[((size_t)(9 + i) * 12 + 3 * X + j) * nblk + o];
+                dst[o] = -s;
+            }
+        }
+#undef BLK
+    for (int a = 0; a < 10; ++a)
+        for (int b = 0; b < 5; ++b)
+            for (int c = 0; c < 5; ++c)
+                for (int d = 0; d < 5; ++d) free(cache[a][b][c][d]);
+    free(v);
+    return 0;
+}
+
+int qxo_shell_quartet_deriv2(const qxo_basis *B, int s1, int s2, int s3, int s4, double *out) {
+    init_tables();
+    return quartet2(B, s1, s2, s3, s4, out);
+}
+
+/* Second-derivative tensor with the reference's semantics
+ * (libint_interface.cc:2582-2779 at deriv_order 2; compute_2e_deriv :1097-1335):
+ * unique nuclear pairs nu1 <= nu2 in the order of generate_multi_index_lookup(3N, 2);
+ * element = sum over shell positions p on atom(nu1), q on atom(nu2) of the
+ * Libint buffer for the sorted pair (3p + c1, 3q + c2).  If pair_idx >= 0 only
+ * that slice is produced. */
+int qxo_eri_deriv2(const qxo_basis *B, double thr, int pair_idx, double *out, int nthreads) {
+    init_tables();
+    int ns = B->nshell, N3 = 3 * B->natom;
+    double *K = (double *)malloc(sizeof(double) * ns * ns);
+    double kmax;
+    qxo_schwarz(B, K, &kmax, nthreads);
+    int *pairs = (int *)malloc(sizeof(int) * ns * (ns + 1));
+    int np = qxo_pairs(B, K, kmax, thr, pairs);
+    long *s2bf = (long *)malloc(sizeof(long) * ns);
+    long n;
+    shell2bf_of(B, s2bf, &n);
+    size_t n4 = (size_t)n * n * n * n;
+    int npair = N3 * (N3 + 1) / 2;
+    int nslice = pair_idx >= 0 ? 1 : npair;
+    memset(out, 0, sizeof(double) * n4 * nslice);
+    int *nu1 = (int *)malloc(sizeof(int) * npair), *nu2 = (int *)malloc(sizeof(int) * npair);
+    for (int a = 0, k = 0; a < N3; ++a)
+        for (int b = a; b < N3; ++b, ++k) { nu1[k] = a; nu2[k] = b; }
+    double thr2 = thr * thr;
+    int nt = nthreads_of(nthreads);
+#pragma omp parallel num_threads(nt)
+    {
+        double *buf = (double *)malloc(sizeof(double) * 1296 * 144);
+#pragma omp for schedule(dynamic)
+        for (int ip = 0; ip < np; ++ip) {
+            int p1 = pairs[2 * ip], p2 = pairs[2 * ip + 1];
+            for (int jp = 0; jp < np; ++jp) {
+                int p3 = pairs[2 * jp], p4 = pairs[2 * jp + 1];
+                if (K[p1 * ns + p2] * K[p3 * ns + p4] < thr2) continue;
+                int at[4] = {B->atom[p1], B->atom[p2], B->atom[p3], B->atom[p4]};
+                if (at[0] == at[1] && at[0] == at[2] && at[0] == at[3]) continue;
+                quartet2(B, p1, p2, p3, p4, buf);
+                int nn[4] = {shell_size(B->l[p1]), shell_size(B->l[p2]), shell_size(B->l[p3]), shell_size(B->l[p4])};
+                size_t nblk = (size_t)nn[0] * nn[1] * nn[2] * nn[3];
+                long b1 = s2bf[p1], b2 = s2bf[p2], b3 = s2bf[p3], b4 = s2bf[p4];
+                for (int s = 0; s < nslice; ++s) {
+                    int k = pair_idx >= 0 ? pair_idx : s;
+                    int A1 = nu1[k] / 3, c1 = nu1[k] % 3, A2 = nu2[k] / 3, c2 = nu2[k] % 3;
+                    int P[4], Q[4], nP = 0, nQ = 0;
+                    for (int c = 0; c < 4; ++c) {
+                        if (at[c] == A1) P[nP++] = 3 * c + c1;
+                        if (at[c] == A2) Q[nQ++] = 3 * c + c2;
+                    }
+                    if (!nP || !nQ) continue;
+                    double *o = out + (size_t)s * n4;
+                    for (int f1 = 0, idx = 0; f1 < nn[0]; ++f1)
+                        for (int f2 = 0; f2 < nn[1]; ++f2)
+                            for (int f3 = 0; f3 < nn[2]; ++f3)
+                                for (int f4 = 0; f4 < nn[3]; ++f4, ++idx) {
+                                    double x = 0.0;
+                                    for (int u = 0; u < nP; ++u)
+                                        for (int w = 0; w < nQ; ++w) {
+                                            int lo = P[u] < Q[w] ? P[u] : Q[w], hi = P[u] < Q[w] ? Q[w] : P[u];
+                                            x += buf[((size_t)lo * 12 + hi) * nblk + idx];
+                                        }
+                                    long i = b1 + f1, j = b2 + f2, kk = b3 + f3, l = b4 + f4;
+                                    o[((i * n + j) * n + kk) * n + l] += x;
+                                    if (p1 != p2) o[((j * n + i) * n + kk) * n + l] += x;
+                                    if (p3 != p4) o[((i * n + j) * n + l) * n + kk] += x;
+                                    if (p1 != p2 && p3 != p4) o[((j * n + i) * n + l) * n + kk] += x;
+                                }
+                }
+            }
+        }
+        free(buf);
+    }
+    free(K); free(pairs); free(s2bf); free(nu1); free(nu2);
+    return 0;
+}
+
 /* Index helpers restated from quax/integrals/utils.h:131-172. */
 int qxo_how_many_derivs(int k, int n) {
     long val = 1, fact = 1;

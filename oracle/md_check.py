@@ -165,3 +165,55 @@ def overlap_xl(shell) -> float:
 
 def normalized(shell):
     return normalize_contraction(shell.l, shell.exps, shell.coefs)
+
+
+def shell_quartet_deriv2(shells):
+    """(12, 12, n1, n2, n3, n4) second derivatives by McMurchie-Davidson, applying the
+    derivative identity on all four centres directly (no translational invariance)."""
+    comps = [cart_components(s.l) for s in shells]
+    coefs = [s.norm_coefs() for s in shells]
+    cen = [np.asarray(s.center, float) for s in shells]
+    shape = tuple(len(c) for c in comps)
+    out = np.zeros((12, 12) + shape)
+    for i1, c1 in enumerate(comps[0]):
+        for i2, c2 in enumerate(comps[1]):
+            for i3, c3 in enumerate(comps[2]):
+                for i4, c4 in enumerate(comps[3]):
+                    ls = [c1, c2, c3, c4]
+                    acc = np.zeros((12, 12))
+                    for p1, a in enumerate(shells[0].exps):
+                        for p2, b in enumerate(shells[1].exps):
+                            for p3, c in enumerate(shells[2].exps):
+                                for p4, d in enumerate(shells[3].exps):
+                                    w = coefs[0][p1] * coefs[1][p2] * coefs[2][p3] * coefs[3][p4]
+                                    ex = [a, b, c, d]
+                                    for P in range(12):
+                                        X, i = divmod(P, 3)
+                                        for Q in range(P, 12):
+                                            Y, j = divmod(Q, 3)
+                                            tot = 0.0
+                                            for fx in (0, 1):
+                                                for fy in (0, 1):
+                                                    lp = [list(t) for t in ls]
+                                                    coef = 1.0
+                                                    if fx == 0:
+                                                        coef *= 2 * ex[X]
+                                                        lp[X][i] += 1
+                                                    else:
+                                                        coef *= -lp[X][i]
+                                                        lp[X][i] -= 1
+                                                    if coef == 0:
+                                                        continue
+                                                    if fy == 0:
+                                                        coef *= 2 * ex[Y]
+                                                        lp[Y][j] += 1
+                                                    else:
+                                                        coef *= -lp[Y][j]
+                                                        lp[Y][j] -= 1
+                                                    if coef == 0 or min(min(t) for t in lp) < 0:
+                                                        continue
+                                                    tot += coef * prim_eri(*[tuple(t) for t in lp], a, b, c, d, *cen)
+                                            acc[P, Q] += w * tot
+                    acc = np.triu(acc) + np.triu(acc, 1).T
+                    out[:, :, i1, i2, i3, i4] = acc
+    return out

@@ -703,10 +703,18 @@ def _warp_targets(la, lb, lc, ld, deriv):
     if not deriv:
         acc = AccSpace("acc", la, lab, lc, lcd)
         return [((e, f), ["acc"]) for e, f in reversed(list(acc.targets()))], {"acc": acc}
-    spaces = {"U": AccSpace("U", la - 1, lab, lc - 1, lcd), "WA": AccSpace("WA", la + 1, lab + 1, lc, lcd),
-              "WB": AccSpace("WB", la, lab + 1, lc, lcd), "WC": AccSpace("WC", la, lab, lc + 1, lcd + 1)}
+    if deriv == 2:
+        spaces = {"U": AccSpace("U", la - 2, lab, lc - 2, lcd), "WA": AccSpace("WA", la, lab + 1, lc - 1, lcd),
+                  "WB": AccSpace("WB", la - 1, lab + 1, lc - 1, lcd), "WC": AccSpace("WC", la - 1, lab, lc, lcd + 1),
+                  "AA": AccSpace("AA", la + 2, lab + 2, lc, lcd), "BB": AccSpace("BB", la, lab + 2, lc, lcd),
+                  "CC": AccSpace("CC", la, lab, lc + 2, lcd + 2), "AB": AccSpace("AB", la + 1, lab + 2, lc, lcd),
+                  "AC": AccSpace("AC", la + 1, lab + 1, lc + 1, lcd + 1),
+                  "BC": AccSpace("BC", la, lab + 1, lc + 1, lcd + 1)}
+    else:
+        spaces = {"U": AccSpace("U", la - 1, lab, lc - 1, lcd), "WA": AccSpace("WA", la + 1, lab + 1, lc, lcd),
+                  "WB": AccSpace("WB", la, lab + 1, lc, lcd), "WC": AccSpace("WC", la, lab, lc + 1, lcd + 1)}
     member = {}
-    for name in ("U", "WA", "WB", "WC"):
+    for name in spaces:
         for t in spaces[name].targets():
             member.setdefault(t, []).append(name)
     order = sorted(member, key=lambda t: (-sum(t[0]), -sum(t[1]), gidx(t[0]), gidx(t[1])))
@@ -736,13 +744,14 @@ def _peak_live(lines, consumed_at):
 
 
 def warp_program(la, lb, lc, ld, deriv):
-    S = la + lb + lc + ld + (1 if deriv else 0)
+    S = la + lb + lc + ld + deriv
     tlist, spaces = _warp_targets(la, lb, lc, ld, deriv)
     em = Emitter("v")
     vr = VRR(em)
     items = []  # (space, e, f)
     leaf = {}
-    wname = {"acc": None, "U": None, "WA": "wa", "WB": "wb", "WC": "wc"}
+    wname = {"acc": None, "U": None, "WA": "wa", "WB": "wb", "WC": "wc", "AA": "wa * wa", "BB": "wb * wb",
+             "CC": "wc * wc", "AB": "wa * wb", "AC": "wa * wc", "BC": "wb * wc"}
     for (e, f), sets in tlist:
         v = vr.get(e, f, 0)
         for sp in sets:
@@ -770,6 +779,65 @@ def warp_program(la, lb, lc, ld, deriv):
         hnodes = sorted(hm.nodes, key=lambda n: n[-1])
         hout = None
         pinned = outs
+    elif deriv == 2:
+        hm = HRRMulti({k: (v, 0) for k, v in spaces.items()})
+        hm.next = nitem_pad
+        hm.leafmap = leaf
+        pairs = [(P, Q) for P in range(9) for Q in range(P, 9)]
+        outs = [None] * (len(pairs) * nout)
+        setname = {(): "U", (0,): "WA", (1,): "WB", (2,): "WC", (0, 0): "AA", (1, 1): "BB", (2, 2): "CC",
+                   (0, 1): "AB", (0, 2): "AC", (1, 2): "BC"}
+        kk = 0
+        for a in comps(la):
+            for b in comps(lb):
+                for c in comps(lc):
+                    for d in comps(ld):
+                        for pi, (P, Q) in enumerate(pairs):
+                            X, i = divmod(P, 3)
+                            Y, j = divmod(Q, 3)
+                            terms = []
+                            for fx in (0, 1):
+                                for fy in (0, 1):
+                                    cm = [list(a), list(b), list(c), list(d)]
+                                    coef = 1
+                                    if fx == 0:
+                                        cm[X][i] += 1
+                                    else:
+                                        coef *= -cm[X][i]
+                                        cm[X][i] -= 1
+                                    if coef == 0:
+                                        continue
+                                    if fy == 0:
+                                        cm[Y][j] += 1
+                                    else:
+                                        coef *= -cm[Y][j]
+                                        cm[Y][j] -= 1
+                                    if coef == 0 or min(min(t) for t in cm) < 0:
+                                        continue
+                                    wset = tuple(sorted(([X] if fx == 0 else []) + ([Y] if fy == 0 else [])))
+                                    terms.append((hm.get(setname[wset], *[tuple(t) for t in cm]), coef))
+                            # merge equal slots, then chain x + c y nodes (constants in -8..7)
+                            merged = {}
+                            for sl, cf in terms:
+                                merged[sl] = merged.get(sl, 0) + cf
+                            terms = [(sl, cf) for sl, cf in merged.items() if cf != 0]
+                            if not terms:
+                                raise RuntimeError("second-derivative output with no terms")
+                            sl0, c0 = terms[0]
+                            node = sl0 if c0 == 1 else hm._new(sl0, sl0, 4, c0 - 1)
+                            for sl, cf in terms[1:]:
+                                node = hm._new(node, sl, 4, cf)
+                            outs[pi * nout + kk] = node
+                        kk += 1
+        owner = {}
+        for ob, sl in enumerate(outs):
+            if sl < nitem_pad or sl in owner:
+                sl = hm._new(sl, sl, 3, 0)
+                outs[ob] = sl
+            owner[sl] = ob
+        hnodes = sorted(hm.nodes, key=lambda n: n[-1])
+        hout = [owner.get(n[0], 0xFFFF) for n in hnodes]
+        pinned = []
     else:
         hm = HRRMulti({k: (v, 0) for k, v in spaces.items()})
         hm.next = nitem_pad
@@ -810,9 +878,18 @@ def warp_feasible(la, lb, lc, ld, deriv):
 
 
 def gen_warp_code(cid, la, lb, lc, ld, deriv, p):
-    tag = f"{'d' if deriv else 'p'}{cid:02d}"
+    tag = f"{'pdh'[deriv]}{cid:02d}"
     L = []
-    hn = [(dst | s1 << 16, s2 | side << 16 | dr << 18) for (dst, s1, s2, side, dr, lvl) in p["hnodes"]]
+    def gidx(side, dr):
+        # geometry / constant slot of the kernel's table: AB 0..2, CD 3..5, 6 + (c + 8) for a constant c
+        if side == 0:
+            return dr
+        if side == 1:
+            return 3 + dr
+        c = -(dr + 1) if side == 2 else (0 if side == 3 else dr)
+        assert -8 <= c <= 7, c
+        return 6 + c + 8
+    hn = [(dst | s1 << 16, s2 | gidx(side, dr) << 16) for (dst, s1, s2, side, dr, lvl) in p["hnodes"]]
     for n in hn:
         assert n[0] < 2**32
     def arr(name, typ, vals, per):
@@ -827,8 +904,8 @@ def gen_warp_code(cid, la, lb, lc, ld, deriv, p):
     L += arr(f"k_hl_{tag}", "int", p["hlev"], str)
     outs = p["outs"]
     L += arr(f"k_ho_{tag}", "unsigned short", outs, str)
-    extra = p["nout"] if deriv else 0
-    smem = p["hslots"] + 16 + extra
+    extra = p["nout"] if deriv == 1 else 0
+    smem = p["hslots"] + 32 + extra
     L.append(f"struct Warp_{tag} {{")
     L.append(f"  static constexpr int LA = {la}, LB = {lb}, LC = {lc}, LD = {ld};")
     L.append(f"  static constexpr int S = {p['S']}, NITEM = {p['nitem']}, NITEM_PAD = {p['nitem_pad']};")
@@ -846,7 +923,7 @@ def gen_warp_code(cid, la, lb, lc, ld, deriv, p):
     L.append("  }")
     L.append("};")
     L.append(f"void qx_launch_warp_{tag}(const qx::WarpArgs& w, int mode, cudaStream_t s) "
-             f"{{ qx::launch_warp<Warp_{tag}, {1 if deriv else 0}>(w, mode, s); }}")
+             f"{{ qx::launch_warp<Warp_{tag}, {deriv}>(w, mode, s); }}")
     return "\n".join(L)
 
 
@@ -898,12 +975,15 @@ def main():
     for fn in os.listdir(os.path.join(here, "gen")):
         if fn.startswith("k_eri_") and fn.endswith(".cu"):
             os.remove(os.path.join(here, "gen", fn))
-    wp, wd = [], []
+    wp, wd, wh = [], [], []
     for i, (a, b, c, d) in enumerate(qc):
         okp, pp = warp_feasible(a, b, c, d, 0)
         okd, pd = warp_feasible(a, b, c, d, 1)
+        okh = max(a, b, c, d) <= 1
+        ph = warp_program(a, b, c, d, 2) if okh else None
         wp.append(okp)
         wd.append(okd)
+        wh.append(okh)
         if (a, b, c, d) in COOP_CLASSES and not okp and not okd:
             continue
         with open(os.path.join(here, "gen", f"k_eri_{i:02d}.cu"), "w") as f:
@@ -917,12 +997,16 @@ def main():
                 f.write(gen_warp_code(i, a, b, c, d, 0, pp) + "\n")
             if okd:
                 f.write(gen_warp_code(i, a, b, c, d, 1, pd) + "\n")
+            if okh:
+                f.write(gen_warp_code(i, a, b, c, d, 2, ph) + "\n")
     with open(os.path.join(here, "gen", "warp_index.cuh"), "w") as f:
         f.write("// Generated by quax_b200/csrc/gen_eri.py -- do not edit by hand.\n#pragma once\n")
         f.write("#define QX_CLASS_WARP_PLAIN {" + ", ".join("1" if x else "0" for x in wp) + "}\n")
         f.write("#define QX_CLASS_WARP_DERIV {" + ", ".join("1" if x else "0" for x in wd) + "}\n")
         f.write("#define QX_FOR_EACH_WARP_PLAIN(X) " + " ".join(f"X({i:02d})" for i, x in enumerate(wp) if x) + "\n")
         f.write("#define QX_FOR_EACH_WARP_DERIV(X) " + " ".join(f"X({i:02d})" for i, x in enumerate(wd) if x) + "\n")
+        f.write("#define QX_CLASS_WARP_DERIV2 {" + ", ".join("1" if x else "0" for x in wh) + "}\n")
+        f.write("#define QX_FOR_EACH_WARP_DERIV2(X) " + " ".join(f"X({i:02d})" for i, x in enumerate(wh) if x) + "\n")
     with open(os.path.join(here, "gen", "der_tables.cuh"), "w") as f:
         f.write(gen_coop_deriv(list(enumerate(qc))))
 

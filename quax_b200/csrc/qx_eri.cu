@@ -53,7 +53,7 @@ static int fail(int code, const char* fmt, ...) {
 extern "C" const char* qx_last_error(void) { return g_err.c_str(); }
 void qx_set_last_error(const char* msg) { g_err = msg; }
 extern "C" int qx_max_l(void) { return QX_GEN_LMAX; }
-extern "C" int qx_max_deriv_order(void) { return 1; }
+extern "C" int qx_max_deriv_order(void) { return 2; }
 
 static constexpr int pair_class(int l1, int l2) { return l1 * (l1 + 1) / 2 + l2; }
 static constexpr int quartet_class(int pb, int pk) { return pb * (pb + 1) / 2 + pk; }
@@ -93,10 +93,13 @@ static const int g_has_warp_plain[QX_NUM_CLASSES] = QX_CLASS_WARP_PLAIN;
 static const int g_has_warp_deriv[QX_NUM_CLASSES] = QX_CLASS_WARP_DERIV;
 static WarpLaunch g_warp_plain[QX_NUM_CLASSES];
 static WarpLaunch g_warp_deriv[QX_NUM_CLASSES];
+static WarpLaunch g_warp_deriv2[QX_NUM_CLASSES];  // second derivatives (classes with l <= 1)
 #define QX_DECL_WP(id) void qx_launch_warp_p##id(const qx::WarpArgs&, int, cudaStream_t);
 QX_FOR_EACH_WARP_PLAIN(QX_DECL_WP)
 #define QX_DECL_WD(id) void qx_launch_warp_d##id(const qx::WarpArgs&, int, cudaStream_t);
 QX_FOR_EACH_WARP_DERIV(QX_DECL_WD)
+#define QX_DECL_WH(id) void qx_launch_warp_h##id(const qx::WarpArgs&, int, cudaStream_t);
+QX_FOR_EACH_WARP_DERIV2(QX_DECL_WH)
 // Engines per class.  Plain ERI: straight-line per-thread kernels (small classes),
 // warp-per-quartet kernels (lanes = primitive quartets), or the cooperative engine
 // (classes whose VRR does not fit a lane's registers).  Derivatives: warp kernels
@@ -109,7 +112,8 @@ long long qx_der_nacc(int der_idx);
 int qx_der_chunk();
 void qx_launch_der(int der_idx, const qx::EriArgs& a, int mode, const double* D, double cj, double ck, double* grad,
                    int slice, cudaStream_t s);
-enum { QX_MODE_DER_DENSE = 10, QX_MODE_DER_SLICE = 11, QX_MODE_GRAD = 12 };
+enum { QX_MODE_DER_DENSE = 10, QX_MODE_DER_SLICE = 11, QX_MODE_GRAD = 12, QX_MODE_DER2_DENSE = 13,
+       QX_MODE_DER2_SLICE = 14 };
 static bool init_class_tables() {
     for (int c = 0; c < QX_NUM_CLASSES; ++c) {
         g_eri_launch[c] = nullptr;
@@ -118,11 +122,14 @@ static bool init_class_tables() {
         g_der_idx[c] = qx_der_index(c);
         g_warp_plain[c] = nullptr;
         g_warp_deriv[c] = nullptr;
+        g_warp_deriv2[c] = nullptr;
     }
 #define QX_SET_WP(id) g_warp_plain[1##id - 100] = &qx_launch_warp_p##id;
     QX_FOR_EACH_WARP_PLAIN(QX_SET_WP)
 #define QX_SET_WD(id) g_warp_deriv[1##id - 100] = &qx_launch_warp_d##id;
     QX_FOR_EACH_WARP_DERIV(QX_SET_WD)
+#define QX_SET_WH(id) g_warp_deriv2[1##id - 100] = &qx_launch_warp_h##id;
+    QX_FOR_EACH_WARP_DERIV2(QX_SET_WH)
 #define QX_SL_ENTRY(id, a, b, c, d)                            \
     g_eri_launch[id] = &qx_launch_eri_##id;                    \
     g_class_scratch[id] = qx::scratch_per_quartet<a, b, c, d>();
@@ -733,6 +740,38 @@ static int run_all_deriv(qx_handle* h, int mode, double* out, const double* D, d
     return QX_OK;
 }
 
+// Second derivatives: every class through its warp order-2 program.  `slice` is
+// 3N for the dense tensor, or the packed nuclear pair nu1 | nu2 << 16 (nu1 <= nu2).
+static int run_all_deriv2(qx_handle* h, int mode, double* out, int slice, cudaStream_t s) {
+    for (int c = 0; c < QX_NUM_CLASSES; ++c)
+        if (h->work[c].nq && !g_warp_deriv2[c])
+            return fail(QX_E_UNSUPPORTED,
+                        "second derivatives: class (%d%d|%d%d) has no order-2 program (this build: s and p shells)",
+                        g_class_l[c][0], g_class_l[c][1], g_class_l[c][2], g_class_l[c][3]);
+    QX_CUDA(cudaEventRecord(h->start, s));
+    for (int i = 0; i < QX_NSTREAMS; ++i) QX_CUDA(cudaStreamWaitEvent(h->streams[i], h->start, 0));
+    int k = 0;
+    for (int oi = 0; oi < QX_NUM_CLASSES; ++oi) {
+        const int c = h->order[oi];
+        if (!h->work[c].nq) continue;
+        cudaStream_t cs = h->streams[k++ % QX_NSTREAMS];
+        WarpArgs wa;
+        wa.e = class_args(h, c, out);
+        wa.wpq = h->wpq[c];
+        wa.D = nullptr;
+        wa.cj = wa.ck = 0.0;
+        wa.grad = nullptr;
+        wa.slice = slice;
+        g_warp_deriv2[c](wa, mode, cs);
+        QX_CUDA(cudaGetLastError());
+    }
+    for (int i = 0; i < QX_NSTREAMS; ++i) {
+        QX_CUDA(cudaEventRecord(h->done[i], h->streams[i]));
+        QX_CUDA(cudaStreamWaitEvent(s, h->done[i], 0));
+    }
+    return QX_OK;
+}
+
 // Stages a host output buffer through the device when out_on_device == 0.
 template <class F>
 static int with_output(qx_handle* h, double* out, size_t count, int out_on_device, cudaStream_t s, F&& body) {
@@ -755,13 +794,16 @@ static int with_output(qx_handle* h, double* out, size_t count, int out_on_devic
 
 extern "C" int qx_eri_deriv_core(qx_handle* h, int order, double* out, int out_on_device, void* stream) {
     if (!h || !out) return fail(QX_E_INVALID, "qx_eri_deriv_core: NULL argument");
-    if (order != 1) return fail(QX_E_UNSUPPORTED, "qx_eri_deriv_core: derivative order %d (this build: 1)", order);
+    if (order < 1 || order > 2)
+        return fail(QX_E_UNSUPPORTED, "qx_eri_deriv_core: derivative order %d (this build: 1 and 2)", order);
     DeviceGuard g(h->device);
     cudaStream_t s = (cudaStream_t)stream;
     const long long n = h->nbf, n4 = n * n * n * n;
-    const size_t count = (size_t)(3 * h->natom) * (size_t)n4;
+    const long long M = 3LL * h->natom;
+    const size_t count = (size_t)(order == 1 ? M : M * (M + 1) / 2) * (size_t)n4;
     return with_output(h, out, count, out_on_device, s, [&](double* d) {
         QX_CUDA(cudaMemsetAsync(d, 0, sizeof(double) * count, s));
+        if (order == 2) return run_all_deriv2(h, QX_MODE_DER2_DENSE, d, (int)M, s);
         return run_all_deriv(h, QX_MODE_DER_DENSE, d, nullptr, 0.0, 0.0, nullptr, -1, s);
     });
 }
@@ -772,20 +814,22 @@ extern "C" int qx_compute_2e_deriv(qx_handle* h, const int* deriv_vec, int len, 
     if (len != 3 * h->natom)
         return fail(QX_E_INVALID, "qx_compute_2e_deriv: deriv_vec has %d entries, expected 3*natom = %d", len,
                     3 * h->natom);
-    int order = 0, idx = -1;
+    int order = 0, nu[2] = {-1, -1};
     for (int i = 0; i < len; ++i) {
         if (deriv_vec[i] < 0) return fail(QX_E_INVALID, "qx_compute_2e_deriv: negative entry in deriv_vec");
+        for (int r = 0; r < deriv_vec[i] && order + r < 2; ++r) nu[order + r] = i;
         order += deriv_vec[i];
-        if (deriv_vec[i]) idx = i;
     }
-    if (order != 1)
-        return fail(QX_E_UNSUPPORTED, "qx_compute_2e_deriv: derivative order %d (this build: 1)", order);
+    if (order < 1 || order > 2)
+        return fail(QX_E_UNSUPPORTED, "qx_compute_2e_deriv: derivative order %d (this build: 1 and 2)", order);
+    if (order == 2 && len > 0xffff) return fail(QX_E_INVALID, "qx_compute_2e_deriv: too many atoms for order 2");
     DeviceGuard g(h->device);
     cudaStream_t s = (cudaStream_t)stream;
     const long long n = h->nbf, n4 = n * n * n * n;
     return with_output(h, out, (size_t)n4, out_on_device, s, [&](double* d) {
         QX_CUDA(cudaMemsetAsync(d, 0, sizeof(double) * n4, s));
-        return run_all_deriv(h, QX_MODE_DER_SLICE, d, nullptr, 0.0, 0.0, nullptr, idx, s);
+        if (order == 2) return run_all_deriv2(h, QX_MODE_DER2_SLICE, d, nu[0] | nu[1] << 16, s);
+        return run_all_deriv(h, QX_MODE_DER_SLICE, d, nullptr, 0.0, 0.0, nullptr, nu[0], s);
     });
 }
 

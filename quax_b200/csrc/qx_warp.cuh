@@ -26,7 +26,7 @@ struct WarpArgs {
 };
 
 enum { WMODE_DENSE = 0, WMODE_UNIQUE = 1, WMODE_SCHWARZ = 2, WMODE_DER_DENSE = 10, WMODE_DER_SLICE = 11,
-       WMODE_GRAD = 12 };
+       WMODE_GRAD = 12, WMODE_DER2_DENSE = 13, WMODE_DER2_SLICE = 14 };
 
 constexpr int WARP_QPB = 4;  // quartets (warps) per block
 
@@ -64,8 +64,9 @@ __device__ __forceinline__ void reduce16(double (&v)[16], double* __restrict__ a
 }
 
 // Table-driven HRR level loop for one warp.  Node (uint2): x = dst | s1<<16,
-// y = s2 | side<<16 | dir<<18 ; V[dst] = V[s1] + g[side,dir] V[s2] with
-// g = AB (side 0), CD (side 1), -(dir+1) (side 2), 0 (side 3).
+// y = s2 | g<<16 ; V[dst] = V[s1] + geo[g] V[s2] with geo = AB_xyz, CD_xyz, then the
+// integer constants -8..7 (linear combinations of shifted blocks in the
+// derivative programs).
 template <class OnOut>
 __device__ __forceinline__ void warp_hrr(const uint2* __restrict__ hn, const int* __restrict__ hl, int nhlev,
                                          const unsigned short* __restrict__ ho, double* H, const double* geo,
@@ -74,9 +75,7 @@ __device__ __forceinline__ void warp_hrr(const uint2* __restrict__ hn, const int
         const int end = __ldg(hl + L + 1);
         for (int nn = __ldg(hl + L) + lane; nn < end; nn += 32) {
             const uint2 d = __ldg(hn + nn);
-            const int side = (d.y >> 16) & 3, dir = (d.y >> 18) & 3;
-            const double g = geo[side < 2 ? 3 * side + dir : (side == 2 ? 6 + dir : 10)];
-            const double v = fma(g, H[d.y & 0xffff], H[d.x >> 16]);
+            const double v = fma(geo[(d.y >> 16) & 31], H[d.y & 0xffff], H[d.x >> 16]);
             H[d.x & 0xffff] = v;
             if (ho) {
                 const int ob = __ldg(ho + nn);
@@ -128,8 +127,8 @@ __global__ void __launch_bounds__(WARP_QPB * 32) k_warp(WarpArgs wa, int mode) {
     if (qi >= a.nq) return;  // whole warp (whole block when wpq = 4)
     extern __shared__ double warp_sm[];
     double* H = warp_sm + (size_t)warp * W::SMEM_PER_WARP;  // accumulators = HRR leaves
-    double* geo = H + W::HSLOTS;                             // 11 geometry / constant factors
-    double* gam = geo + 16;                                  // adjoint: Gamma weights (NOUT)
+    double* geo = H + W::HSLOTS;                             // 6 geometry factors + constants -8..7
+    double* gam = geo + 32;                                  // adjoint: Gamma weights (NOUT)
     const int2 pq = a.quartets[qi];
     const PairInfo P = a.pairs[pq.x];
     const PairInfo Q = a.pairs[pq.y];
@@ -139,6 +138,12 @@ __global__ void __launch_bounds__(WARP_QPB * 32) k_warp(WarpArgs wa, int mode) {
         if (mode == WMODE_DER_SLICE) {
             const int sa = wa.slice / 3;
             if (atA != sa && atB != sa && atC != sa && atD != sa) return;
+        }
+        if (mode == WMODE_DER2_SLICE) {
+            const int s1 = wa.slice & 0xffff, s2 = wa.slice >> 16;  // nuclear indices nu1 <= nu2
+            const int a1 = s1 / 3, a2 = s2 / 3;
+            if ((atA != a1 && atB != a1 && atC != a1 && atD != a1) || (atA != a2 && atB != a2 && atC != a2 && atD != a2))
+                return;
         }
     }
     for (int t = lane; t < W::NITEM_PAD; t += 32) H[t] = 0.0;
@@ -176,12 +181,12 @@ __global__ void __launch_bounds__(WARP_QPB * 32) k_warp(WarpArgs wa, int mode) {
     if (lane == 0) {
         geo[0] = P.ABx; geo[1] = P.ABy; geo[2] = P.ABz;
         geo[3] = Q.ABx; geo[4] = Q.ABy; geo[5] = Q.ABz;
-        geo[6] = -1.0; geo[7] = -2.0; geo[8] = -3.0; geo[9] = -4.0; geo[10] = 0.0;
     }
+    if (lane < 16) geo[6 + lane] = (double)((int)lane - 8);
     constexpr int NB = ncart_h(W::LB), NC = ncart_h(W::LC), ND = ncart_h(W::LD);
     const bool s12 = P.s1 != P.s2, s34 = Q.s1 != Q.s2, sPQ = pq.x != pq.y;
     const long long n = a.n;
-    if (DERIV && mode == WMODE_GRAD) {
+    if (DERIV == 1 && mode == WMODE_GRAD) {
         const double* __restrict__ Dm = wa.D;
         const double fJ = (1.0 + sPQ) * (1.0 + s12) * (1.0 + s34), fK = 1.0 + sPQ;
         const double kd = 1.0 + (double)(s12 && s34), kx = (double)s12 + (double)s34;
@@ -219,6 +224,45 @@ __global__ void __launch_bounds__(WARP_QPB * 32) k_warp(WarpArgs wa, int mode) {
                 dense_images(a.out, n, P.bf1 + ia, P.bf2 + ib, Q.bf1 + ic, Q.bf2 + id, s12, s34, sPQ, H[__ldg(outs + o)]);
             }
         }
+        return;
+    }
+    if (DERIV == 2) {
+        // 45 independent blocks h[U,V], U = 3X+i <= V = 3Y+j over the A, B, C
+        // coordinates; with D = -(A+B+C) each h[U,V] adds to the nuclear Hessian
+        // entries (U,V), (D_i,V), (U,D_j), (D_i,D_j) with signs +, -, -, +, for both
+        // orderings of an off-diagonal block; an entry is kept in the unique
+        // (nu1 <= nu2) slot of the reference's pair numbering.
+        const int atoms[4] = {atA, atB, atC, atD};
+        const long long n4 = n * n * n * n;
+        const int M = wa.slice;  // dense: 3N; slice mode: packed pair (nu1 | nu2 << 16)
+        warp_hrr(W::hnodes(), W::hlev(), W::NHLEV, W::outs(), H, geo, lane, [&](int ob, double v) {
+            int pidx = ob / W::NOUT;
+            const int o = ob - pidx * W::NOUT;
+            int Pc = 0;
+            while (pidx >= 9 - Pc) {
+                pidx -= 9 - Pc;
+                ++Pc;
+            }
+            const int Qc = Pc + pidx;
+            const int id = o % ND, ic = (o / ND) % NC, ib = (o / (ND * NC)) % NB, ia = o / (ND * NC * NB);
+            const long long ii = P.bf1 + ia, jj = P.bf2 + ib, kk = Q.bf1 + ic, ll = Q.bf2 + id;
+            for (int ord = 0; ord < (Pc == Qc ? 1 : 2); ++ord) {
+                const int U = ord ? Qc : Pc, V = ord ? Pc : Qc;
+                const int xu = U / 3, iu = U % 3, xv = V / 3, iv = V % 3;
+                for (int su = 0; su < 2; ++su)
+                    for (int sv = 0; sv < 2; ++sv) {
+                        const int nu1 = 3 * atoms[su ? 3 : xu] + iu, nu2 = 3 * atoms[sv ? 3 : xv] + iv;
+                        if (nu1 > nu2) continue;
+                        const double c = ((su + sv) & 1) ? -v : v;
+                        if (mode == WMODE_DER2_DENSE) {
+                            const long long rank = (long long)nu1 * M - (long long)nu1 * (nu1 - 1) / 2 + (nu2 - nu1);
+                            atomic_images_w(a.out + rank * n4, n, ii, jj, kk, ll, s12, s34, sPQ, c);
+                        } else if (nu1 == (M & 0xffff) && nu2 == (M >> 16)) {
+                            atomic_images_w(a.out, n, ii, jj, kk, ll, s12, s34, sPQ, c);
+                        }
+                    }
+            }
+        });
         return;
     }
     // derivative programs: the epilogue runs at each output node

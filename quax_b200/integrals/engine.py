@@ -13,6 +13,7 @@ import numpy as np
 import torch
 
 from ..basis import Basis
+from ..utils import how_many_derivs
 from . import _lib
 
 
@@ -142,9 +143,10 @@ class EriEngine:
 
     # -- derivatives ----------------------------------------------------------
     def eri_deriv_core(self, order: int = 1, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
-        """Dense (3N, n, n, n, n) first-derivative tensor on the device (reference layout)."""
+        """Dense derivative tensor on the device, reference layout: (3N, n, n, n, n) for
+        order 1, (3N(3N+1)/2, n, n, n, n) for order 2 (nuclear pairs nu1 <= nu2)."""
         n = self.nbf
-        shape = (3 * self.natom, n, n, n, n)
+        shape = (how_many_derivs(self.natom, int(order)), n, n, n, n)
         if out is None:
             out = torch.empty(shape, dtype=torch.float64, device=self.device)
         with torch.cuda.device(self.device):

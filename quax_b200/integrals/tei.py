@@ -25,6 +25,7 @@ import numpy as np
 import torch
 
 from ..utils import get_deriv_vec_idx, how_many_derivs
+from . import _lib
 from .engine import EriEngine
 
 
@@ -41,11 +42,14 @@ class TEI:
             raise ValueError(f"unknown mode {mode}")
         self.eri_derivatives = []
         if mode == "core" and max_deriv_order > 0:
-            if max_deriv_order > 1:
-                raise NotImplementedError("precomputed derivative tensors of order > 1")
-            d = self.engine.eri_deriv_core(1)
-            assert d.shape[0] == how_many_derivs(self.natom, 1)
-            self.eri_derivatives.append(d)
+            # tei.py:29-34: one tensor of unique derivatives per order
+            top = _lib.load().qx_max_deriv_order()
+            if max_deriv_order > top:
+                raise NotImplementedError(f"precomputed derivative tensors of order {max_deriv_order} (this build: {top})")
+            for k in range(1, max_deriv_order + 1):
+                d = self.engine.eri_deriv_core(k)
+                assert d.shape[0] == how_many_derivs(self.natom, k)
+                self.eri_derivatives.append(d)
 
     def eri(self, geom=None) -> torch.Tensor:
         return self.engine.eri()

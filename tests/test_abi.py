@@ -32,7 +32,7 @@ def test_build_info():
 
     lib = _lib.load()
     assert lib.qx_max_l() == 2
-    assert lib.qx_max_deriv_order() == 1
+    assert lib.qx_max_deriv_order() == 2
     assert lib.qx_num_classes() == 21
 
 

@@ -80,13 +80,81 @@ def test_grad_adjoint_matches_oracle_and_plain(oracle_lib, seed):
     assert np.abs(g.reshape(-1, 3).sum(axis=0)).max() < 1e-9
 
 
-def test_deriv_errors():
-    b = small_synthetic(0)
+def sp_synthetic(seed, natom=3, kmax=3):
+    spec = SyntheticSpec(natom=natom, box=5.0, min_sep=1.2, kmax=kmax, exp_lo=0.1, exp_hi=50.0,
+                         heavy_ls=(0, 0, 1, 1), h_ls=(0, 1))
+    return synthetic_molecule(spec, seed)[1]
+
+
+def test_h2o_deriv2_core(oracle_lib):
+    b = build_basis(h2o_config1(), "sto-3g")
+    eng = _engine(b, 1e-14)
+    d = eng.eri_deriv_core(2).cpu().numpy()
+    ref = oracle_lib.eri_deriv2(oracle_lib.OracleBasis(b), 1e-14)
+    assert d.shape == (45, 7, 7, 7, 7)
+    assert np.abs(d - ref).max() < ATOL_D * max(1.0, np.abs(ref).max())
+
+
+@pytest.mark.parametrize("seed", [0, 3])
+def test_synthetic_deriv2_core(oracle_lib, seed):
+    b = sp_synthetic(seed)
     eng = _engine(b, 1e-12)
+    d = eng.eri_deriv_core(2).cpu().numpy()
+    ref = oracle_lib.eri_deriv2(oracle_lib.OracleBasis(b), 1e-12)
+    assert np.abs(d - ref).max() < ATOL_D * max(1.0, np.abs(ref).max())
+    # symmetry of each slice under the 8 permutations of (ij|kl)
+    assert np.abs(d - d.transpose(0, 2, 1, 3, 4)).max() < 1e-13 * max(1.0, np.abs(d).max())
+    assert np.abs(d - d.transpose(0, 3, 4, 1, 2)).max() < 1e-13 * max(1.0, np.abs(d).max())
+
+
+def test_deriv2_slices(oracle_lib):
+    from quax_b200.utils import get_deriv_vec_idx
+
+    b = sp_synthetic(5, natom=4)
+    eng = _engine(b, 1e-12)
+    ob = oracle_lib.OracleBasis(b)
+    M = 3 * b.natom
+    full = eng.eri_deriv_core(2).cpu().numpy()
+    for nu1, nu2 in ((0, 0), (0, 1), (2, 7), (4, M - 1), (M - 1, M - 1)):
+        dv = np.zeros(M, dtype=int)
+        dv[nu1] += 1
+        dv[nu2] += 1
+        s = eng.eri_deriv(dv).cpu().numpy()
+        r = get_deriv_vec_idx(dv)
+        ref = oracle_lib.eri_deriv2(ob, 1e-12, pair_idx=r)
+        assert np.abs(s - ref).max() < ATOL_D * max(1.0, np.abs(ref).max())
+        assert np.abs(s - full[r]).max() < 1e-13 * max(1.0, np.abs(ref).max())
+
+
+def test_deriv2_translational_invariance():
+    # sum over the atoms of one Cartesian direction of d^2/dnu1 dnu2 vanishes
+    b = sp_synthetic(2)
+    eng = _engine(b, 1e-12)
+    M = 3 * b.natom
+    d = eng.eri_deriv_core(2).cpu().numpy()
+    H = np.zeros((M, M) + d.shape[1:])
+    r = 0
+    for a in range(M):
+        for c in range(a, M):
+            H[a, c] = H[c, a] = d[r]
+            r += 1
+    for x in range(3):
+        s = H[x::3].sum(axis=0)
+        assert np.abs(s).max() < 1e-10 * max(1.0, np.abs(d).max())
+
+
+def test_deriv_errors():
+    b = small_synthetic(0)  # carries d shells
+    eng = _engine(b, 1e-12)
+    with pytest.raises(NotImplementedError):
+        eng.eri_deriv_core(order=3)
     with pytest.raises(NotImplementedError):
         eng.eri_deriv_core(order=2)
     dv = np.zeros(3 * b.natom, dtype=int)
     dv[0] = 2
+    with pytest.raises(NotImplementedError):
+        eng.eri_deriv(dv)
+    dv[0] = 3
     with pytest.raises(NotImplementedError):
         eng.eri_deriv(dv)
     with pytest.raises(ValueError):

@@ -115,3 +115,30 @@ def test_gradient_oracle_matches_dense_contraction(oracle_lib):
     g_dense = np.einsum("xijkl,ijkl->x", oracle_lib.eri_deriv1(ob, 1e-14), Gam)
     g = oracle_lib.grad_contract(ob, 1e-14, D, 1.0, -0.5)
     assert np.abs(g - g_dense).max() < 1e-12
+
+
+@pytest.mark.parametrize("ls", [(0, 0, 0, 0), (1, 0, 0, 0), (1, 1, 0, 1)])
+def test_second_derivatives_mcmurchie_davidson(oracle_lib, ls):
+    sh = _random_shells(50 + sum(ls), ls, k=1)
+    o = oracle_lib.shell_quartet_deriv2(oracle_lib.OracleBasis(Basis(sh, 4)), 0, 1, 2, 3)
+    m = md_check.shell_quartet_deriv2(sh)
+    assert np.abs(o - m).max() < 1e-12 * max(1.0, np.abs(m).max())
+
+
+def test_second_derivative_tensor_against_finite_differences(oracle_lib):
+    """d/dR_nu2 of the first-derivative slice nu1, five-point differences (h = 1e-3)."""
+    mol = h2o_config1()
+    b = build_basis(mol, "sto-3g")
+    d2 = oracle_lib.eri_deriv2(oracle_lib.OracleBasis(b), 1e-14)
+    assert d2.shape == (45, 7, 7, 7, 7)
+    from quax_b200.utils import multiset_rank
+
+    h = 1e-3
+    for nu1, nu2 in [(0, 0), (0, 4), (2, 7), (5, 5)]:
+        def d1(shift):
+            c = mol.coords.copy()
+            c.flat[nu2] += shift
+            return oracle_lib.eri_deriv1(oracle_lib.OracleBasis(b.with_coords(c)), 1e-14, deriv_idx=nu1)
+        fd = (d1(-2 * h) - 8 * d1(-h) + 8 * d1(h) - d1(2 * h)) / (12 * h)
+        k = multiset_rank(sorted((nu1, nu2)), 9)
+        assert np.abs(d2[k] - fd).max() < 5e-8
