@@ -144,6 +144,27 @@ int qx_class_info(const qx_handle *h, int cls, int *l4, long long *nquartets, lo
 /* qx_eri_unique restricted to one class (same output positions). */
 int qx_eri_unique_class(qx_handle *h, int cls, double *out_dev, void *stream);
 
+/* qx_grad_adjoint restricted to one class: adds that class's contribution into
+ * grad_dev (3N doubles, device memory; not zeroed here).  D_dev is n x n on the
+ * device.  For per-class timing and engine tuning. */
+int qx_grad_adjoint_class(qx_handle *h, int cls, const double *D_dev, double cj, double ck, double *grad_dev,
+                          void *stream);
+
+/* Autotuner, no counterpart in the reference.  Times, on this handle's own
+ * quartet lists, every engine configuration each class can run and keeps the
+ * fastest: straight-line kernels with 1..32 lanes per quartet, warp kernels with
+ * 1 or 4 warps per quartet, the warp-VRR + cooperative-HRR pair, the cooperative
+ * engines.  what: bit 0 = plain ERI (timed in unique mode), bit 1 = first
+ * derivatives (timed in adjoint-gradient mode).  Synchronises `stream`;
+ * allocates and frees its own scratch. */
+int qx_autotune(qx_handle *h, int what, void *stream);
+
+/* Engine configuration of one class: cfg[0] plain engine (0 straight-line,
+ * 1 warp, 2 cooperative), cfg[1] its parameter (log2 lanes per quartet, or warps
+ * per quartet), cfg[2] derivative engine (1 warp, 2 cooperative, 3 warp VRR into
+ * global accumulators + cooperative HRR), cfg[3] its warps per quartet. */
+int qx_engine_config(const qx_handle *h, int cls, int *cfg);
+
 /* Size of the fixed device array qx_compute_2e_int_noalloc works in. */
 #define QX_NOALLOC_SCRATCH_BYTES (16u << 20)
 

@@ -743,32 +743,112 @@ def _peak_live(lines, consumed_at):
     return pk
 
 
-def warp_program(la, lb, lc, ld, deriv):
-    S = la + lb + lc + ld + deriv
-    tlist, spaces = _warp_targets(la, lb, lc, ld, deriv)
+# Live VRR values (doubles, two registers each) one chunk of a derivative
+# program may keep.  Straight-line code above that spills to local memory; below
+# it the program is cut into chunks that each recompute the intermediates they
+# need from the saved inputs (see qx_load_inputs), so no chunk's values outlive it.
+WARP_LIVE_BUDGET = {0: None, 1: 80, 2: None}
+
+_TARGET_ORDERS = {
+    # highest bra AM first (the order of the plain programs)
+    "bra_desc": lambda t: (-sum(t[0]), -sum(t[1]), gidx(t[0]), gidx(t[1])),
+    # lowest bra AM first: fewer live values per chunk for the derivative programs
+    "bra_asc": lambda t: (sum(t[0]), gidx(t[0]), sum(t[1]), gidx(t[1])),
+}
+
+
+def _chunk_cost(tl):
+    """(FP ops, peak live values) of the straight-line VRR for the targets tl."""
     em = Emitter("v")
     vr = VRR(em)
+    for (e, f), sets in tl:
+        v = vr.get(e, f, 0)
+        for _ in sets:
+            em.lines.append(f"stg[0] = {v};")
+    ops = sum(ln.count("*") + ln.count(" + ") + ln.count(" - ") for ln in em.lines if ln.startswith("const"))
+    return ops, _peak_live(em.lines, None)
+
+
+def _chunks(tl, budget):
+    """Greedy cut of tl into contiguous chunks whose peak live count fits the budget."""
+    out, s = [], 0
+    while s < len(tl):
+        lo, hi = s + 1, len(tl)
+        while lo < hi:
+            mid = (lo + hi + 1) // 2
+            if _chunk_cost(tl[s:mid])[1] <= budget:
+                lo = mid
+            else:
+                hi = mid - 1
+        out.append((s, lo))
+        s = lo
+    return out
+
+
+def _plan_targets(tlist, budget):
+    """Target order and chunk bounds: one chunk if it fits, else the order with the
+    fewest recomputed operations."""
+    if budget is None or _chunk_cost(tlist)[1] <= budget:
+        return tlist, [(0, len(tlist))]
+    best = None
+    for key in _TARGET_ORDERS.values():
+        tl = sorted(tlist, key=lambda x: key(x[0]))
+        ch = _chunks(tl, budget)
+        ops = sum(_chunk_cost(tl[a:b])[0] for a, b in ch)
+        if best is None or ops < best[0]:
+            best = (ops, tl, ch)
+    return best[1], best[2]
+
+
+def warp_program(la, lb, lc, ld, deriv):
+    import re as _re
+    S = la + lb + lc + ld + deriv
+    tlist, spaces = _warp_targets(la, lb, lc, ld, deriv)
+    tlist, chunks = _plan_targets(tlist, WARP_LIVE_BUDGET[deriv])
     items = []  # (space, e, f)
     leaf = {}
     wname = {"acc": None, "U": None, "WA": "wa", "WB": "wb", "WC": "wc", "AA": "wa * wa", "BB": "wb * wb",
              "CC": "wc * wc", "AB": "wa * wb", "AC": "wa * wc", "BC": "wb * wc"}
-    for (e, f), sets in tlist:
-        v = vr.get(e, f, 0)
-        for sp in sets:
-            k = len(items)
-            items.append((sp, e, f))
-            leaf[(sp, e, f)] = k
-            w = wname[sp]
-            em.lines.append(f"stg[{k % 16}] = {v};" if w is None else f"stg[{k % 16}] = {w} * {v};")
-            if k % 16 == 15:
-                em.lines.append(f"reduce16(stg, acc + {k - 15}, lane);")
+    lines = []
+    peak = 0
+    for ci, (c0, c1) in enumerate(chunks):
+        em = Emitter(f"v{ci}_" if len(chunks) > 1 else "v")
+        vr = VRR(em)
+        for (e, f), sets in tlist[c0:c1]:
+            v = vr.get(e, f, 0)
+            for sp in sets:
+                k = len(items)
+                items.append((sp, e, f))
+                leaf[(sp, e, f)] = k
+                w = wname[sp]
+                em.lines.append(f"stg[{k % 16}] = {v};" if w is None else f"stg[{k % 16}] = {w} * {v};")
+                if k % 16 == 15:
+                    em.lines.append(f"sink(stg, {k - 15}, lane);")
+        peak = max(peak, _peak_live(em.lines, None))
+        if ci == 0:
+            if len(chunks) > 1:
+                lines.append(f"qx_save_inputs<{S + 1}>(q, Fp, save, lane);")
+            lines += em.lines
+        else:
+            # the inputs again, by volatile loads of the lane's saved copy: the
+            # compiler cannot merge this chunk's intermediates with an earlier
+            # chunk's, whose values are dead by now
+            lines.append("{")
+            lines.append(f"  double Fc[{S + 1}];")
+            lines.append("  PrimQ qc;")
+            lines.append(f"  qx_load_inputs<{S + 1}>(save, lane, qc, Fc);")
+            for ln in em.lines:
+                ln = ln.replace("Fp[", "Fc[")
+                lines.append("  " + _re.sub(r"\bq\.", "qc.", ln))
+            lines.append("}")
+    em = Emitter("v")
+    em.lines = lines
     nitem = len(items)
     if nitem % 16:
         for k in range(nitem, (nitem + 15) // 16 * 16):
             em.lines.append(f"stg[{k % 16}] = 0.0;")
-        em.lines.append(f"reduce16(stg, acc + {(nitem // 16) * 16}, lane);")
+        em.lines.append(f"sink(stg, {(nitem // 16) * 16}, lane);")
     nitem_pad = (nitem + 15) // 16 * 16
-    peak = _peak_live(em.lines, None)
     # HRR over the item layout
     nout = ncart(la) * ncart(lb) * ncart(lc) * ncart(ld)
     if not deriv:
@@ -868,16 +948,48 @@ def warp_program(la, lb, lc, ld, deriv):
     hlev = [sum(1 for n in hnodes if n[-1] < lv) for lv in range(1, max((n[-1] for n in hnodes), default=0) + 1)]
     hlev.append(len(hnodes))
     hnodes2, pinned2, hslots = _realloc([(n[0], n[1:3], n[-1]) for n in hnodes], hnodes, pinned, nitem_pad, "h")
+    vmap = None
+    if deriv == 1:
+        # item -> accumulator index of the cooperative derivative layout (spaces
+        # U, WA, WB, WC back to back), for the global-accumulator VRR kernel
+        offs, o = {}, 0
+        for name in ("U", "WA", "WB", "WC"):
+            offs[name] = o
+            o += spaces[name].size
+        vmap = [offs[sp] + spaces[sp].index(e, f) for sp, e, f in items] + [0xFFFF] * (nitem_pad - nitem)
     return dict(S=S, lines=em.lines, nitem=nitem, nitem_pad=nitem_pad, peak=peak, hnodes=hnodes2, hlev=hlev,
-                outs=pinned2 if not deriv else hout, hslots=max(hslots, nitem_pad), nout=nout)
+                outs=pinned2 if not deriv else hout, hslots=max(hslots, nitem_pad), nout=nout, vmap=vmap,
+                nchunk=len(chunks))
 
 
 def warp_feasible(la, lb, lc, ld, deriv):
     p = warp_program(la, lb, lc, ld, deriv)
-    return p["peak"] <= WARP_PEAK_MAX, p
+    return p["peak"] <= WARP_PEAK_MAX and warp_smem(p, deriv) <= WARP_SMEM_MAX, p
 
 
-def gen_warp_code(cid, la, lb, lc, ld, deriv, p):
+def wvrr_wanted(la, lb, lc, ld):
+    """Classes that also get the global-accumulator derivative VRR kernel: the ones
+    with long primitive loops and large accumulator sets."""
+    return la + lb + lc + ld >= 6
+
+
+WARP_SMEM_MAX = (227 * 1024) // (8 * 4)  # doubles of shared memory per warp (4 warps per block)
+
+
+def warp_save(p):
+    """Per-warp input save area (doubles) of a chunked program: 17 PrimQ scalars and
+    S + 1 Boys values per lane."""
+    return (17 + p["S"] + 1) * 32 if p["nchunk"] > 1 else 0
+
+
+def warp_smem(p, deriv):
+    return p["hslots"] + 32 + (p["nout"] if deriv == 1 else 0) + warp_save(p)
+
+
+def gen_warp_code(cid, la, lb, lc, ld, deriv, p, want_warp=True, want_wvrr=False):
+    """Warp program of one class: the k_warp kernel (accumulators in shared memory,
+    HRR and epilogue in the same kernel) and/or, for first derivatives, the
+    global-accumulator VRR kernel k_wvrr that feeds the cooperative HRR pass."""
     tag = f"{'pdh'[deriv]}{cid:02d}"
     L = []
     def gidx(side, dr):
@@ -889,9 +1001,6 @@ def gen_warp_code(cid, la, lb, lc, ld, deriv, p):
         c = -(dr + 1) if side == 2 else (0 if side == 3 else dr)
         assert -8 <= c <= 7, c
         return 6 + c + 8
-    hn = [(dst | s1 << 16, s2 | gidx(side, dr) << 16) for (dst, s1, s2, side, dr, lvl) in p["hnodes"]]
-    for n in hn:
-        assert n[0] < 2**32
     def arr(name, typ, vals, per):
         out = [f"static __device__ const {typ} {name}[{max(len(vals), 1)}] = {{"]
         for i0 in range(0, len(vals), 8):
@@ -900,30 +1009,44 @@ def gen_warp_code(cid, la, lb, lc, ld, deriv, p):
             out.append("  {}" if typ.startswith("uint") else "  0")
         out.append("};")
         return out
-    L += arr(f"k_hn_{tag}", "uint2", hn, lambda v: "{%du,%du}" % v)
-    L += arr(f"k_hl_{tag}", "int", p["hlev"], str)
-    outs = p["outs"]
-    L += arr(f"k_ho_{tag}", "unsigned short", outs, str)
-    extra = p["nout"] if deriv == 1 else 0
-    smem = p["hslots"] + 32 + extra
+    if want_warp:
+        hn = [(dst | s1 << 16, s2 | gidx(side, dr) << 16) for (dst, s1, s2, side, dr, lvl) in p["hnodes"]]
+        for n in hn:
+            assert n[0] < 2**32
+        L += arr(f"k_hn_{tag}", "uint2", hn, lambda v: "{%du,%du}" % v)
+        L += arr(f"k_hl_{tag}", "int", p["hlev"], str)
+        L += arr(f"k_ho_{tag}", "unsigned short", p["outs"], str)
+    if want_wvrr:
+        assert p["vmap"] is not None and max(p["vmap"]) <= 0xFFFF
+        L += arr(f"k_vm_{tag}", "unsigned short", p["vmap"], str)
     L.append(f"struct Warp_{tag} {{")
     L.append(f"  static constexpr int LA = {la}, LB = {lb}, LC = {lc}, LD = {ld};")
     L.append(f"  static constexpr int S = {p['S']}, NITEM = {p['nitem']}, NITEM_PAD = {p['nitem_pad']};")
     L.append(f"  static constexpr int HSLOTS = {p['hslots']}, NOUT = {p['nout']}, NHLEV = {len(p['hlev']) - 1};")
-    L.append(f"  static constexpr int SMEM_PER_WARP = {smem};")
-    L.append(f"  static __device__ __forceinline__ const uint2* hnodes() {{ return k_hn_{tag}; }}")
-    L.append(f"  static __device__ __forceinline__ const int* hlev() {{ return k_hl_{tag}; }}")
-    L.append(f"  static __device__ __forceinline__ const unsigned short* outs() {{ return k_ho_{tag}; }}")
-    L.append("  template <class Q>")
+    L.append(f"  static constexpr int SMEM_PER_WARP = {warp_smem(p, deriv)};")
+    L.append(f"  static constexpr int NCHUNK = {p['nchunk']};  // VRR chunks (recomputed intermediates)")
+    L.append(f"  static constexpr int SAVE = {warp_save(p)};  // per-warp input save area (doubles)")
+    if want_warp:
+        L.append(f"  static __device__ __forceinline__ const uint2* hnodes() {{ return k_hn_{tag}; }}")
+        L.append(f"  static __device__ __forceinline__ const int* hlev() {{ return k_hl_{tag}; }}")
+        L.append(f"  static __device__ __forceinline__ const unsigned short* outs() {{ return k_ho_{tag}; }}")
+    if want_wvrr:
+        L.append(f"  static __device__ __forceinline__ const unsigned short* vmap() {{ return k_vm_{tag}; }}")
+    L.append("  template <class Q, class Sink>")
     L.append("  static __device__ __forceinline__ void vrr(const double* __restrict__ Fp, const Q& q, double wa, double wb,"
-             " double wc, double* __restrict__ acc, unsigned lane) {")
-    L.append("    (void)wa; (void)wb; (void)wc;")
+             " double wc, const Sink& sink, unsigned lane, double* save) {")
+    L.append("    (void)wa; (void)wb; (void)wc; (void)save;")
     L.append("    double stg[16];")
     L += ["    " + ln for ln in p["lines"]]
     L.append("  }")
     L.append("};")
-    L.append(f"void qx_launch_warp_{tag}(const qx::WarpArgs& w, int mode, cudaStream_t s) "
-             f"{{ qx::launch_warp<Warp_{tag}, {deriv}>(w, mode, s); }}")
+    if want_warp:
+        L.append(f"void qx_launch_warp_{tag}(const qx::WarpArgs& w, int mode, cudaStream_t s) "
+                 f"{{ qx::launch_warp<Warp_{tag}, {deriv}>(w, mode, s); }}")
+    if want_wvrr:
+        L.append(f"void qx_launch_wvrr_{tag}(const qx::EriArgs& a, const int2* tasks, long long ntask, int chunk, "
+                 f"double* acc, int nacc, cudaStream_t s) "
+                 f"{{ qx::launch_wvrr<Warp_{tag}>(a, tasks, ntask, chunk, acc, nacc, s); }}")
     return "\n".join(L)
 
 
@@ -975,16 +1098,18 @@ def main():
     for fn in os.listdir(os.path.join(here, "gen")):
         if fn.startswith("k_eri_") and fn.endswith(".cu"):
             os.remove(os.path.join(here, "gen", fn))
-    wp, wd, wh = [], [], []
+    wp, wd, wh, wv = [], [], [], []
     for i, (a, b, c, d) in enumerate(qc):
         okp, pp = warp_feasible(a, b, c, d, 0)
         okd, pd = warp_feasible(a, b, c, d, 1)
+        okv = wvrr_wanted(a, b, c, d) and pd["peak"] <= WARP_PEAK_MAX
         okh = max(a, b, c, d) <= 1
         ph = warp_program(a, b, c, d, 2) if okh else None
         wp.append(okp)
         wd.append(okd)
         wh.append(okh)
-        if (a, b, c, d) in COOP_CLASSES and not okp and not okd:
+        wv.append(okv)
+        if (a, b, c, d) in COOP_CLASSES and not okp and not okd and not okv:
             continue
         with open(os.path.join(here, "gen", f"k_eri_{i:02d}.cu"), "w") as f:
             f.write("// Generated by quax_b200/csrc/gen_eri.py -- do not edit by hand.\n")
@@ -995,8 +1120,8 @@ def main():
                 f.write(f"QX_DEFINE_LAUNCH({i}, {a}, {b}, {c}, {d})\n")
             if okp:
                 f.write(gen_warp_code(i, a, b, c, d, 0, pp) + "\n")
-            if okd:
-                f.write(gen_warp_code(i, a, b, c, d, 1, pd) + "\n")
+            if okd or okv:
+                f.write(gen_warp_code(i, a, b, c, d, 1, pd, want_warp=okd, want_wvrr=okv) + "\n")
             if okh:
                 f.write(gen_warp_code(i, a, b, c, d, 2, ph) + "\n")
     with open(os.path.join(here, "gen", "warp_index.cuh"), "w") as f:
@@ -1005,6 +1130,8 @@ def main():
         f.write("#define QX_CLASS_WARP_DERIV {" + ", ".join("1" if x else "0" for x in wd) + "}\n")
         f.write("#define QX_FOR_EACH_WARP_PLAIN(X) " + " ".join(f"X({i:02d})" for i, x in enumerate(wp) if x) + "\n")
         f.write("#define QX_FOR_EACH_WARP_DERIV(X) " + " ".join(f"X({i:02d})" for i, x in enumerate(wd) if x) + "\n")
+        f.write("#define QX_CLASS_WVRR {" + ", ".join("1" if x else "0" for x in wv) + "}\n")
+        f.write("#define QX_FOR_EACH_WVRR(X) " + " ".join(f"X({i:02d})" for i, x in enumerate(wv) if x) + "\n")
         f.write("#define QX_CLASS_WARP_DERIV2 {" + ", ".join("1" if x else "0" for x in wh) + "}\n")
         f.write("#define QX_FOR_EACH_WARP_DERIV2(X) " + " ".join(f"X({i:02d})" for i, x in enumerate(wh) if x) + "\n")
     with open(os.path.join(here, "gen", "der_tables.cuh"), "w") as f:

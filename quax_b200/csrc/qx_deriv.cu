@@ -316,6 +316,28 @@ void qx_launch_der_split(int der_idx, const qx::EriArgs& a, int mode, const doub
     k_der<<<(unsigned)a.nq, da.W * 32, smem, s>>>(da, mode);
 }
 
+// HRR and epilogue from accumulator sums that another kernel produced (the
+// warp-program VRR of the largest classes): acc holds nq * nacc doubles in this
+// engine's accumulator layout.
+void qx_launch_der_hrr(int der_idx, const qx::EriArgs& a, int mode, const double* D, double cj, double ck,
+                       double* grad, int slice, const double* acc, cudaStream_t s) {
+    using namespace qx;
+    DerArgs da;
+    da.e = a;
+    da.c = g_der_classes[der_idx];
+    da.D = D;
+    da.cj = cj;
+    da.ck = ck;
+    da.grad = grad;
+    da.slice = slice;
+    da.acc_in = acc;
+    if (!a.nq) return;
+    size_t smem;
+    der_plan_hrr(da.c, da.W, da.region, smem);
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_der, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_der<<<(unsigned)a.nq, da.W * 32, smem, s>>>(da, mode);
+}
+
 long long qx_der_nacc(int der_idx) { return g_der_classes[der_idx].nacc; }
 int qx_der_chunk() { return qx::DER_CHUNK; }
 

@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -91,25 +92,32 @@ static int g_der_idx[QX_NUM_CLASSES];
 static const int g_class_nacc[QX_NUM_CLASSES] = QX_CLASS_NACC;
 static const int g_has_warp_plain[QX_NUM_CLASSES] = QX_CLASS_WARP_PLAIN;
 static const int g_has_warp_deriv[QX_NUM_CLASSES] = QX_CLASS_WARP_DERIV;
+static const int g_has_wvrr[QX_NUM_CLASSES] = QX_CLASS_WVRR;
 static WarpLaunch g_warp_plain[QX_NUM_CLASSES];
 static WarpLaunch g_warp_deriv[QX_NUM_CLASSES];
 static WarpLaunch g_warp_deriv2[QX_NUM_CLASSES];  // second derivatives (classes with l <= 1)
+static WvrrLaunch g_wvrr[QX_NUM_CLASSES];          // derivative VRR into global accumulators
 #define QX_DECL_WP(id) void qx_launch_warp_p##id(const qx::WarpArgs&, int, cudaStream_t);
 QX_FOR_EACH_WARP_PLAIN(QX_DECL_WP)
 #define QX_DECL_WD(id) void qx_launch_warp_d##id(const qx::WarpArgs&, int, cudaStream_t);
 QX_FOR_EACH_WARP_DERIV(QX_DECL_WD)
 #define QX_DECL_WH(id) void qx_launch_warp_h##id(const qx::WarpArgs&, int, cudaStream_t);
 QX_FOR_EACH_WARP_DERIV2(QX_DECL_WH)
+#define QX_DECL_WV(id) \
+    void qx_launch_wvrr_d##id(const qx::EriArgs&, const int2*, long long, int, double*, int, cudaStream_t);
+QX_FOR_EACH_WVRR(QX_DECL_WV)
 // Engines per class.  Plain ERI: straight-line per-thread kernels (small classes),
 // warp-per-quartet kernels (lanes = primitive quartets), or the cooperative engine
 // (classes whose VRR does not fit a lane's registers).  Derivatives: warp kernels
 // where they fit, else the cooperative derivative engine.
-enum { ENG_SL = 0, ENG_WARP = 1, ENG_COOP = 2 };
+enum { ENG_SL = 0, ENG_WARP = 1, ENG_COOP = 2, ENG_WVRR = 3 };
 int qx_der_index(int cls);
 void qx_launch_der_split(int der_idx, const qx::EriArgs& a, int mode, const double* D, double cj, double ck,
                          double* grad, int slice, const int2* tasks, long long ntask, double* scratch, cudaStream_t s);
 long long qx_der_nacc(int der_idx);
 int qx_der_chunk();
+void qx_launch_der_hrr(int der_idx, const qx::EriArgs& a, int mode, const double* D, double cj, double ck,
+                       double* grad, int slice, const double* acc, cudaStream_t s);
 void qx_launch_der(int der_idx, const qx::EriArgs& a, int mode, const double* D, double cj, double ck, double* grad,
                    int slice, cudaStream_t s);
 enum { QX_MODE_DER_DENSE = 10, QX_MODE_DER_SLICE = 11, QX_MODE_GRAD = 12, QX_MODE_DER2_DENSE = 13,
@@ -123,6 +131,7 @@ static bool init_class_tables() {
         g_warp_plain[c] = nullptr;
         g_warp_deriv[c] = nullptr;
         g_warp_deriv2[c] = nullptr;
+        g_wvrr[c] = nullptr;
     }
 #define QX_SET_WP(id) g_warp_plain[1##id - 100] = &qx_launch_warp_p##id;
     QX_FOR_EACH_WARP_PLAIN(QX_SET_WP)
@@ -130,6 +139,8 @@ static bool init_class_tables() {
     QX_FOR_EACH_WARP_DERIV(QX_SET_WD)
 #define QX_SET_WH(id) g_warp_deriv2[1##id - 100] = &qx_launch_warp_h##id;
     QX_FOR_EACH_WARP_DERIV2(QX_SET_WH)
+#define QX_SET_WV(id) g_wvrr[1##id - 100] = &qx_launch_wvrr_d##id;
+    QX_FOR_EACH_WVRR(QX_SET_WV)
 #define QX_SL_ENTRY(id, a, b, c, d)                            \
     g_eri_launch[id] = &qx_launch_eri_##id;                    \
     g_class_scratch[id] = qx::scratch_per_quartet<a, b, c, d>();
@@ -229,8 +240,8 @@ struct qx_handle {
     int order[QX_NUM_CLASSES];  // classes by decreasing primitive work
     int plain_eng[QX_NUM_CLASSES];
     int deriv_eng[QX_NUM_CLASSES];
-    int wpq[QX_NUM_CLASSES];  // warps per quartet for the warp kernels
-    std::vector<int2> lists_host[QX_NUM_CLASSES];  // kept for lazily built derivative tasks
+    int wpq[QX_NUM_CLASSES];        // warps per quartet, plain warp kernels
+    int wpq_deriv[QX_NUM_CLASSES];  // warps per quartet, derivative warp kernels
 };
 
 // Primitive-chunk tasks and accumulator sums of the derivative split mode, built
@@ -238,7 +249,8 @@ struct qx_handle {
 static int ensure_deriv_tasks(qx_handle* h, int c) {
     ClassWork& w = h->work[c];
     if (w.d_dtasks || !w.nq) return QX_OK;
-    const auto& L = h->lists_host[c];
+    std::vector<int2> L((size_t)w.nq);
+    QX_CUDA(cudaMemcpy(L.data(), w.d_q, sizeof(int2) * w.nq, cudaMemcpyDeviceToHost));
     std::vector<int2> tasks;
     const int ch = qx_der_chunk();
     for (size_t qi = 0; qi < L.size(); ++qi) {
@@ -278,8 +290,9 @@ static void choose_engines(qx_handle* h) {
             if (!std::strcmp(pe, "warp") && g_has_warp_plain[c]) p = ENG_WARP;
             if (!std::strcmp(pe, "coop") && g_class_coop[c]) p = ENG_COOP;
         }
-        int d = g_has_warp_deriv[c] ? ENG_WARP : ENG_COOP;
+        int d = g_has_warp_deriv[c] ? ENG_WARP : (g_has_wvrr[c] ? ENG_WVRR : ENG_COOP);
         if (de && !std::strcmp(de, "coop")) d = ENG_COOP;
+        if (de && !std::strcmp(de, "wvrr") && g_has_wvrr[c]) d = ENG_WVRR;
         h->plain_eng[c] = p;
         h->deriv_eng[c] = d;
     }
@@ -364,7 +377,7 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
     qx_handle* h = new qx_handle();
     cudaGetDevice(&h->device);
     choose_engines(h);
-    for (int c = 0; c < QX_NUM_CLASSES; ++c) h->wpq[c] = 1;
+    for (int c = 0; c < QX_NUM_CLASSES; ++c) h->wpq[c] = h->wpq_deriv[c] = 1;
     h->natom = natom;
     h->nshell = nshell;
     h->pure = pure;
@@ -557,14 +570,13 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
         w.nq = (long long)sorted.size();
         w.prims = prims;
         w.log2g = h->plain_eng[c] == ENG_SL ? choose_log2g(w.nq, prims) : 0;
-        h->wpq[c] = choose_wpq(w.nq, prims);
+        h->wpq[c] = h->wpq_deriv[c] = choose_wpq(w.nq, prims);
         w.unique_base = base;
         base += w.nq * g_class_nout[c];
         h->nunique += w.nq;
         if (w.nq) {
             QX_ALLOC(w.d_q, sizeof(int2) * w.nq);
             cudaMemcpy(w.d_q, sorted.data(), sizeof(int2) * w.nq, cudaMemcpyHostToDevice);
-            if (h->deriv_eng[c] == ENG_COOP) h->lists_host[c] = sorted;  // tasks built on first use
             if (g_class_scratch[c] && h->plain_eng[c] == ENG_SL)
                 QX_ALLOC(w.scratch, sizeof(double) * g_class_scratch[c] * launch_threads(w.nq, w.log2g));
         }
@@ -702,6 +714,41 @@ static EriArgs class_args(qx_handle* h, int c, double* out) {
     return a;
 }
 
+// One class through its first-derivative engine on stream `cs`.
+static int run_deriv_class(qx_handle* h, int c, int mode, double* out, const double* D, double cj, double ck,
+                           double* grad, int slice, cudaStream_t cs) {
+    if (h->deriv_eng[c] == ENG_WARP) {
+        WarpArgs wa;
+        wa.e = class_args(h, c, out);
+        wa.wpq = h->wpq_deriv[c];
+        wa.D = D;
+        wa.cj = cj;
+        wa.ck = ck;
+        wa.grad = grad;
+        wa.slice = slice;
+        g_warp_deriv[c](wa, mode, cs);
+    } else if (h->deriv_eng[c] == ENG_WVRR) {
+        // warp-program VRR into global accumulators, then the cooperative HRR pass
+        int rc = ensure_deriv_tasks(h, c);
+        if (rc) return rc;
+        const ClassWork& w = h->work[c];
+        const long long nacc = qx_der_nacc(g_der_idx[c]);
+        QX_CUDA(cudaMemsetAsync(w.d_dacc, 0, sizeof(double) * w.nq * nacc, cs));
+        const EriArgs a = class_args(h, c, out);
+        g_wvrr[c](a, w.d_dtasks, w.ndtask, qx_der_chunk(), w.d_dacc, (int)nacc, cs);
+        qx_launch_der_hrr(g_der_idx[c], a, mode, D, cj, ck, grad, slice, w.d_dacc, cs);
+    } else {
+        if (g_der_idx[c] < 0) return fail(QX_E_UNSUPPORTED, "no derivative program for class %d", c);
+        int rc = ensure_deriv_tasks(h, c);
+        if (rc) return rc;
+        const ClassWork& w = h->work[c];
+        qx_launch_der_split(g_der_idx[c], class_args(h, c, out), mode, D, cj, ck, grad, slice, w.d_dtasks,
+                            w.ndtask, w.d_dacc, cs);
+    }
+    QX_CUDA(cudaGetLastError());
+    return QX_OK;
+}
+
 // Every class through the derivative engine on the internal streams, joined
 // back into `s`.
 static int run_all_deriv(qx_handle* h, int mode, double* out, const double* D, double cj, double ck, double* grad,
@@ -712,26 +759,8 @@ static int run_all_deriv(qx_handle* h, int mode, double* out, const double* D, d
     for (int oi = 0; oi < QX_NUM_CLASSES; ++oi) {
         const int c = h->order[oi];
         if (!h->work[c].nq) continue;
-        cudaStream_t cs = h->streams[k++ % QX_NSTREAMS];
-        if (h->deriv_eng[c] == ENG_WARP) {
-            WarpArgs wa;
-            wa.e = class_args(h, c, out);
-            wa.wpq = h->wpq[c];
-            wa.D = D;
-            wa.cj = cj;
-            wa.ck = ck;
-            wa.grad = grad;
-            wa.slice = slice;
-            g_warp_deriv[c](wa, mode, cs);
-        } else {
-            if (g_der_idx[c] < 0) return fail(QX_E_UNSUPPORTED, "no derivative program for class %d", c);
-            int rc = ensure_deriv_tasks(h, c);
-            if (rc) return rc;
-            const ClassWork& w = h->work[c];
-            qx_launch_der_split(g_der_idx[c], class_args(h, c, out), mode, D, cj, ck, grad, slice, w.d_dtasks,
-                                w.ndtask, w.d_dacc, cs);
-        }
-        QX_CUDA(cudaGetLastError());
+        int rc = run_deriv_class(h, c, mode, out, D, cj, ck, grad, slice, h->streams[k++ % QX_NSTREAMS]);
+        if (rc) return rc;
     }
     for (int i = 0; i < QX_NSTREAMS; ++i) {
         QX_CUDA(cudaEventRecord(h->done[i], h->streams[i]));
@@ -757,7 +786,7 @@ static int run_all_deriv2(qx_handle* h, int mode, double* out, int slice, cudaSt
         cudaStream_t cs = h->streams[k++ % QX_NSTREAMS];
         WarpArgs wa;
         wa.e = class_args(h, c, out);
-        wa.wpq = h->wpq[c];
+        wa.wpq = h->wpq_deriv[c];
         wa.D = nullptr;
         wa.cj = wa.ck = 0.0;
         wa.grad = nullptr;
@@ -891,6 +920,152 @@ extern "C" int qx_eri_unique_class(qx_handle* h, int cls, double* out_dev, void*
     if (!w.nq) return QX_OK;
     return run_class(h, cls, MODE_UNIQUE, w.d_q, w.nq, out_dev, 0, w.unique_base, (cudaStream_t)stream, w.log2g,
                      w.scratch);
+}
+
+extern "C" int qx_grad_adjoint_class(qx_handle* h, int cls, const double* D_dev, double cj, double ck,
+                                     double* grad_dev, void* stream) {
+    if (!h || !D_dev || !grad_dev || cls < 0 || cls >= QX_NUM_CLASSES)
+        return fail(QX_E_INVALID, "qx_grad_adjoint_class: bad argument");
+    DeviceGuard g(h->device);
+    if (!h->work[cls].nq) return QX_OK;
+    return run_deriv_class(h, cls, QX_MODE_GRAD, nullptr, D_dev, cj, ck, grad_dev, -1, (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------- autotuner ----
+// Times every engine configuration a class can run (straight-line with 1..32
+// lanes per quartet, warp kernels with 1 or 4 warps per quartet, the warp-VRR +
+// cooperative-HRR pair, the cooperative engines) on this handle's own quartet
+// lists and keeps the fastest.  Plain configurations are timed in unique-ERI
+// mode, derivative ones in adjoint-gradient mode.  All engines compute the same
+// sums, in different orders, so the choice changes results only by rounding.
+namespace {
+struct TuneCfg {
+    int eng, param;  // param: log2g (straight-line) or warps per quartet (warp)
+};
+}  // namespace
+
+static int time_config(cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1, float* best_ms,
+                       const std::function<int()>& launch) {
+    int rc = launch();  // warm-up (lazy allocations, kernel attributes)
+    if (rc) return rc;
+    float best = 1e30f;
+    for (int r = 0; r < 3; ++r) {
+        QX_CUDA(cudaEventRecord(e0, s));
+        rc = launch();
+        if (rc) return rc;
+        QX_CUDA(cudaEventRecord(e1, s));
+        QX_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        QX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        best = std::min(best, ms);
+    }
+    *best_ms = best;
+    return QX_OK;
+}
+
+extern "C" int qx_autotune(qx_handle* h, int what, void* stream) {
+    if (!h || (what & ~3) || !what) return fail(QX_E_INVALID, "qx_autotune: bad argument");
+    DeviceGuard g(h->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    long long max_out = 0;
+    for (int c = 0; c < QX_NUM_CLASSES; ++c) max_out = std::max(max_out, h->work[c].nq * (long long)g_class_nout[c]);
+    const long long n = h->nbf;
+    double *d_out = nullptr, *d_D = nullptr, *d_g = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int rc = QX_OK;
+    if (cudaMalloc((void**)&d_out, sizeof(double) * std::max(1LL, max_out)) != cudaSuccess ||
+        cudaMalloc((void**)&d_D, sizeof(double) * n * n) != cudaSuccess ||
+        cudaMalloc((void**)&d_g, sizeof(double) * 3 * h->natom) != cudaSuccess) {
+        cudaGetLastError();
+        rc = fail(QX_E_NOMEM, "qx_autotune: scratch allocation failed");
+    }
+    if (!rc && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
+        rc = fail(QX_E_CUDA, "qx_autotune: event creation failed");
+    // a positive density (every byte 0x3f: 4.8e-4 in each entry)
+    if (!rc && cudaMemsetAsync(d_D, 0x3f, sizeof(double) * n * n, s) != cudaSuccess)
+        rc = fail(QX_E_CUDA, "qx_autotune: memset failed");
+    if (!rc && cudaMemsetAsync(d_g, 0, sizeof(double) * 3 * h->natom, s) != cudaSuccess)
+        rc = fail(QX_E_CUDA, "qx_autotune: memset failed");
+    for (int c = 0; c < QX_NUM_CLASSES && !rc; ++c) {
+        ClassWork& w = h->work[c];
+        if (!w.nq) continue;
+        if (what & 1) {
+            std::vector<TuneCfg> cand;
+            if (!g_class_coop[c] && !g_class_scratch[c])
+                for (int lg = 0; lg <= 5; ++lg) cand.push_back({ENG_SL, lg});
+            if (g_has_warp_plain[c]) {
+                cand.push_back({ENG_WARP, 1});
+                cand.push_back({ENG_WARP, 4});
+            }
+            if (g_class_coop[c]) cand.push_back({ENG_COOP, 0});
+            const int keep_wpq = h->wpq[c], keep_lg = w.log2g;
+            float best = 1e30f;
+            TuneCfg bc{h->plain_eng[c], h->plain_eng[c] == ENG_SL ? keep_lg : keep_wpq};
+            for (const TuneCfg& t : cand) {
+                h->plain_eng[c] = t.eng;
+                if (t.eng == ENG_WARP) h->wpq[c] = t.param;
+                const int lg = t.eng == ENG_SL ? t.param : 0;
+                float ms = 0.f;
+                rc = time_config(s, e0, e1, &ms, [&] {
+                    return run_class(h, c, MODE_UNIQUE, w.d_q, w.nq, d_out, 0, 0, s, lg, w.scratch);
+                });
+                if (rc) break;
+                if (ms < best) {
+                    best = ms;
+                    bc = t;
+                }
+            }
+            h->plain_eng[c] = bc.eng;
+            h->wpq[c] = bc.eng == ENG_WARP ? bc.param : keep_wpq;
+            w.log2g = bc.eng == ENG_SL ? bc.param : keep_lg;
+        }
+        if ((what & 2) && !rc) {
+            std::vector<TuneCfg> cand;
+            if (g_has_warp_deriv[c]) {
+                cand.push_back({ENG_WARP, 1});
+                cand.push_back({ENG_WARP, 4});
+            }
+            if (g_has_wvrr[c]) cand.push_back({ENG_WVRR, 0});
+            if (g_der_idx[c] >= 0) cand.push_back({ENG_COOP, 0});
+            float best = 1e30f;
+            TuneCfg bc{h->deriv_eng[c], h->wpq_deriv[c]};
+            for (const TuneCfg& t : cand) {
+                h->deriv_eng[c] = t.eng;
+                if (t.eng == ENG_WARP) h->wpq_deriv[c] = t.param;
+                float ms = 0.f;
+                rc = time_config(s, e0, e1, &ms, [&] {
+                    return run_deriv_class(h, c, QX_MODE_GRAD, nullptr, d_D, 1.0, -0.5, d_g, -1, s);
+                });
+                if (rc) break;
+                if (ms < best) {
+                    best = ms;
+                    bc = t;
+                }
+            }
+            h->deriv_eng[c] = bc.eng;
+            if (bc.eng == ENG_WARP) h->wpq_deriv[c] = bc.param;
+        }
+    }
+    if (!rc) {
+        cudaError_t e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) rc = fail(QX_E_CUDA, "qx_autotune: %s", cudaGetErrorString(e));
+    }
+    if (!rc) rc = check_err_word(h, s);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(d_out);
+    cudaFree(d_D);
+    cudaFree(d_g);
+    return rc;
+}
+
+extern "C" int qx_engine_config(const qx_handle* h, int cls, int* cfg) {
+    if (!h || !cfg || cls < 0 || cls >= QX_NUM_CLASSES) return fail(QX_E_INVALID, "qx_engine_config: bad argument");
+    cfg[0] = h->plain_eng[cls];
+    cfg[1] = h->plain_eng[cls] == ENG_SL ? h->work[cls].log2g : (h->plain_eng[cls] == ENG_WARP ? h->wpq[cls] : 0);
+    cfg[2] = h->deriv_eng[cls];
+    cfg[3] = h->deriv_eng[cls] == ENG_WARP ? h->wpq_deriv[cls] : 0;
+    return QX_OK;
 }
 
 // ---------------------------------------------------------------- direct J/K ---

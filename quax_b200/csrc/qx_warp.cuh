@@ -30,8 +30,9 @@ enum { WMODE_DENSE = 0, WMODE_UNIQUE = 1, WMODE_SCHWARZ = 2, WMODE_DER_DENSE = 1
 
 constexpr int WARP_QPB = 4;  // quartets (warps) per block
 
-// Sum item k of the 16 staged values over the warp; lane 2j ends with item j.
-__device__ __forceinline__ void reduce16(double (&v)[16], double* __restrict__ acc16, unsigned lane) {
+// Sum item k of the 16 staged values over the warp; lane 2j ends with item j
+// (in v[0]).
+__device__ __forceinline__ void reduce16_core(double (&v)[16], unsigned lane) {
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
         const bool up = lane & 16;
@@ -60,7 +61,63 @@ __device__ __forceinline__ void reduce16(double (&v)[16], double* __restrict__ a
         v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
     }
     v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
+}
+
+__device__ __forceinline__ void reduce16(double (&v)[16], double* __restrict__ acc16, unsigned lane) {
+    reduce16_core(v, lane);
     if (!(lane & 1)) acc16[(lane >> 1) & 15] += v[0];
+}
+
+// Where a warp program's staged items go: the warp's shared-memory accumulators
+// (item order), or a quartet's global accumulators through an item -> slot map
+// (atomic adds: several warps share a quartet).
+struct SmemSink {
+    double* acc;
+    __device__ __forceinline__ void operator()(double (&v)[16], int base, unsigned lane) const {
+        reduce16(v, acc + base, lane);
+    }
+};
+
+struct GlobalSink {
+    double* acc;
+    const unsigned short* map;
+    __device__ __forceinline__ void operator()(double (&v)[16], int base, unsigned lane) const {
+        reduce16_core(v, lane);
+        if (!(lane & 1)) {
+            const unsigned m = __ldg(map + base + (lane >> 1));
+            if (m != 0xFFFFu) atomicAdd(acc + m, v[0]);
+        }
+    }
+};
+
+// Chunked warp programs: the lane's VRR inputs are saved once per primitive
+// quartet (lane-strided, bank-conflict free) and every later chunk reloads them
+// with volatile loads, so the compiler cannot merge a chunk's recomputed
+// intermediates with an earlier chunk's and keep them all live.
+template <int NF>
+__device__ __forceinline__ void qx_save_inputs(const PrimQ& q, const double* Fp, double* save, unsigned lane) {
+    double* s = save + lane;
+    s[0 * 32] = q.PAx; s[1 * 32] = q.PAy; s[2 * 32] = q.PAz;
+    s[3 * 32] = q.WPx; s[4 * 32] = q.WPy; s[5 * 32] = q.WPz;
+    s[6 * 32] = q.QCx; s[7 * 32] = q.QCy; s[8 * 32] = q.QCz;
+    s[9 * 32] = q.WQx; s[10 * 32] = q.WQy; s[11 * 32] = q.WQz;
+    s[12 * 32] = q.oo2z; s[13 * 32] = q.roz; s[14 * 32] = q.oo2e;
+    s[15 * 32] = q.roe; s[16 * 32] = q.oo2ze;
+#pragma unroll
+    for (int m = 0; m < NF; ++m) s[(17 + m) * 32] = Fp[m];
+}
+
+template <int NF>
+__device__ __forceinline__ void qx_load_inputs(const double* save, unsigned lane, PrimQ& q, double* F) {
+    const volatile double* s = save + lane;
+    q.PAx = s[0 * 32]; q.PAy = s[1 * 32]; q.PAz = s[2 * 32];
+    q.WPx = s[3 * 32]; q.WPy = s[4 * 32]; q.WPz = s[5 * 32];
+    q.QCx = s[6 * 32]; q.QCy = s[7 * 32]; q.QCz = s[8 * 32];
+    q.WQx = s[9 * 32]; q.WQy = s[10 * 32]; q.WQz = s[11 * 32];
+    q.oo2z = s[12 * 32]; q.roz = s[13 * 32]; q.oo2e = s[14 * 32];
+    q.roe = s[15 * 32]; q.oo2ze = s[16 * 32];
+#pragma unroll
+    for (int m = 0; m < NF; ++m) F[m] = s[(17 + m) * 32];
 }
 
 // Table-driven HRR level loop for one warp.  Node (uint2): x = dst | s1<<16,
@@ -129,6 +186,7 @@ __global__ void __launch_bounds__(WARP_QPB * 32) k_warp(WarpArgs wa, int mode) {
     double* H = warp_sm + (size_t)warp * W::SMEM_PER_WARP;  // accumulators = HRR leaves
     double* geo = H + W::HSLOTS;                             // 6 geometry factors + constants -8..7
     double* gam = geo + 32;                                  // adjoint: Gamma weights (NOUT)
+    double* save = H + (W::SMEM_PER_WARP - W::SAVE);         // chunked VRR: saved lane inputs
     const int2 pq = a.quartets[qi];
     const PairInfo P = a.pairs[pq.x];
     const PairInfo Q = a.pairs[pq.y];
@@ -163,7 +221,7 @@ __global__ void __launch_bounds__(WARP_QPB * 32) k_warp(WarpArgs wa, int mode) {
 #pragma unroll
             for (int m = 0; m <= W::S; ++m) Fp[m] = 0.0;
         }
-        W::vrr(Fp, q, 2.0 * p.alpha, 2.0 * (p.zeta - p.alpha), 2.0 * r.alpha, H, lane);
+        W::vrr(Fp, q, 2.0 * p.alpha, 2.0 * (p.zeta - p.alpha), 2.0 * r.alpha, SmemSink{H}, lane, save);
         __syncwarp();
     }
     if (wpq > 1) {
@@ -319,5 +377,56 @@ void launch_warp(const WarpArgs& wa, int mode, cudaStream_t s) {
 }
 
 typedef void (*WarpLaunch)(const WarpArgs&, int mode, cudaStream_t);
+
+// Derivative VRR of one (quartet, primitive chunk) task per warp into the
+// quartet's global accumulators (cooperative derivative layout), which the
+// cooperative HRR pass then turns into integrals.  For the largest classes, whose
+// accumulators and HRR slots do not fit a warp's shared memory.  acc must be
+// zeroed before the launch.
+template <class W>
+__global__ void __launch_bounds__(WARP_QPB * 32) k_wvrr(EriArgs a, const int2* __restrict__ tasks, long long ntask,
+                                                         int chunk, double* __restrict__ acc, int nacc) {
+    const unsigned lane = threadIdx.x & 31;
+    const long long ti = (long long)blockIdx.x * WARP_QPB + (threadIdx.x >> 5);
+    if (ti >= ntask) return;  // whole warp
+    const int2 task = tasks[ti];
+    const int2 pq = a.quartets[task.x];
+    const PairInfo P = a.pairs[pq.x];
+    const PairInfo Q = a.pairs[pq.y];
+    if (P.atom1 == P.atom2 && P.atom1 == Q.atom1 && P.atom1 == Q.atom2) return;  // reference skips these
+    const GlobalSink sink{acc + (size_t)task.x * nacc, W::vmap()};
+    extern __shared__ double wv_sm[];
+    double* save = wv_sm + (size_t)(threadIdx.x >> 5) * W::SAVE;
+    const int nk = Q.nprim, ntot = P.nprim * nk;
+    const int tend = min(ntot, task.y + chunk);
+    for (int t0 = task.y; t0 < tend; t0 += 32) {
+        const int t = t0 + (int)lane;
+        const bool act = t < tend;
+        const int tt = act ? t : task.y;
+        const int i = tt / nk, j = tt - i * nk;
+        const PrimPair p = a.prims[P.prim_off + i];
+        const PrimPair r = a.prims[Q.prim_off + j];
+        PrimQ q;
+        double Fp[W::S + 1];
+        prim_setup<W::S>(p, r, a.boys, q, Fp);
+        if (!act) {
+#pragma unroll
+            for (int m = 0; m <= W::S; ++m) Fp[m] = 0.0;
+        }
+        W::vrr(Fp, q, 2.0 * p.alpha, 2.0 * (p.zeta - p.alpha), 2.0 * r.alpha, sink, lane, save);
+        __syncwarp();
+    }
+}
+
+template <class W>
+void launch_wvrr(const EriArgs& a, const int2* tasks, long long ntask, int chunk, double* acc, int nacc,
+                 cudaStream_t s) {
+    const long long nb = (ntask + WARP_QPB - 1) / WARP_QPB;
+    const size_t smem = sizeof(double) * (size_t)W::SAVE * WARP_QPB;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_wvrr<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (nb) k_wvrr<W><<<(unsigned)nb, WARP_QPB * 32, smem, s>>>(a, tasks, ntask, chunk, acc, nacc);
+}
+
+typedef void (*WvrrLaunch)(const EriArgs&, const int2*, long long, int, double*, int, cudaStream_t);
 
 }  // namespace qx

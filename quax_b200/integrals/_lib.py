@@ -52,6 +52,9 @@ SIGNATURES = {
         [_vp, C.c_int, _ip, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), _dp, _dp],
     ),
     "qx_eri_unique_class": (C.c_int, [_vp, C.c_int, _vp, _vp]),
+    "qx_grad_adjoint_class": (C.c_int, [_vp, C.c_int, _vp, C.c_double, C.c_double, _vp, _vp]),
+    "qx_autotune": (C.c_int, [_vp, C.c_int, _vp]),
+    "qx_engine_config": (C.c_int, [_vp, C.c_int, _vp]),
     "qx_compute_2e_int_noalloc": (
         C.c_int,
         [C.c_int, _dp, C.c_int, _ip, _ip, _ip, _dp, _dp, C.c_double, _vp, _vp],

@@ -141,6 +141,38 @@ class EriEngine:
             )
         return out
 
+    ENGINE_NAMES = ("sl", "warp", "coop", "wvrr")
+
+    def autotune(self, plain: bool = True, deriv: bool = True, stream=None) -> None:
+        """Time every engine configuration per class on this molecule and keep the fastest."""
+        what = (1 if plain else 0) | (2 if deriv else 0)
+        with torch.cuda.device(self.device):
+            _lib.check(_lib.load().qx_autotune(self.handle, what, C.c_void_p(_stream_ptr(stream))), "qx_autotune")
+
+    def engine_config(self):
+        """{"la lb lc ld": (plain engine, param, deriv engine, param)} for the classes with quartets."""
+        lib = _lib.load()
+        out = {}
+        for c in self.class_info():
+            if not c["nq"]:
+                continue
+            cfg = np.zeros(4, dtype=np.int32)
+            _lib.check(lib.qx_engine_config(self.handle, c["cls"], C.c_void_p(cfg.ctypes.data)), "qx_engine_config")
+            out["%d%d%d%d" % c["l"]] = (self.ENGINE_NAMES[cfg[0]], int(cfg[1]), self.ENGINE_NAMES[cfg[2]], int(cfg[3]))
+        return out
+
+    def grad_adjoint_class(self, cls: int, D: torch.Tensor, grad: torch.Tensor, cj: float = 1.0, ck: float = -0.5,
+                           stream=None) -> torch.Tensor:
+        """Adds one class's adjoint-gradient contribution into grad (3N, device)."""
+        with torch.cuda.device(self.device):
+            _lib.check(
+                _lib.load().qx_grad_adjoint_class(self.handle, int(cls), C.c_void_p(D.data_ptr()), float(cj),
+                                                  float(ck), C.c_void_p(grad.data_ptr()),
+                                                  C.c_void_p(_stream_ptr(stream))),
+                "qx_grad_adjoint_class",
+            )
+        return grad
+
     # -- derivatives ----------------------------------------------------------
     def eri_deriv_core(self, order: int = 1, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
         """Dense derivative tensor on the device, reference layout: (3N, n, n, n, n) for
