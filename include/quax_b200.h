@@ -160,8 +160,9 @@ int qx_grad_adjoint_class(qx_handle *h, int cls, const double *D_dev, double cj,
 int qx_autotune(qx_handle *h, int what, void *stream);
 
 /* Engine configuration of one class: cfg[0] plain engine (0 straight-line,
- * 1 warp, 2 cooperative), cfg[1] its parameter (log2 lanes per quartet, or warps
- * per quartet), cfg[2] derivative engine (1 warp, 2 cooperative, 3 warp VRR into
+ * 1 warp, 2 cooperative, 4 warp VRR into global accumulators + warp HRR),
+ * cfg[1] its parameter (log2 lanes per quartet, or warps per quartet), cfg[2]
+ * derivative engine (1 warp, 2 cooperative, 3 warp VRR into
  * global accumulators + cooperative HRR), cfg[3] its warps per quartet. */
 int qx_engine_config(const qx_handle *h, int cls, int *cfg);
 

@@ -970,6 +970,11 @@ def warp_feasible(la, lb, lc, ld, deriv):
 def wvrr_wanted(la, lb, lc, ld):
     """Classes that also get the global-accumulator derivative VRR kernel: the ones
     with long primitive loops and large accumulator sets."""
+    return la + lb + lc + ld >= 4
+
+
+def pvrr_wanted(la, lb, lc, ld):
+    """Classes that also get the global-accumulator plain VRR kernel (split mode)."""
     return la + lb + lc + ld >= 6
 
 
@@ -1016,7 +1021,7 @@ def gen_warp_code(cid, la, lb, lc, ld, deriv, p, want_warp=True, want_wvrr=False
         L += arr(f"k_hn_{tag}", "uint2", hn, lambda v: "{%du,%du}" % v)
         L += arr(f"k_hl_{tag}", "int", p["hlev"], str)
         L += arr(f"k_ho_{tag}", "unsigned short", p["outs"], str)
-    if want_wvrr:
+    if want_wvrr and deriv:
         assert p["vmap"] is not None and max(p["vmap"]) <= 0xFFFF
         L += arr(f"k_vm_{tag}", "unsigned short", p["vmap"], str)
     L.append(f"struct Warp_{tag} {{")
@@ -1030,7 +1035,7 @@ def gen_warp_code(cid, la, lb, lc, ld, deriv, p, want_warp=True, want_wvrr=False
         L.append(f"  static __device__ __forceinline__ const uint2* hnodes() {{ return k_hn_{tag}; }}")
         L.append(f"  static __device__ __forceinline__ const int* hlev() {{ return k_hl_{tag}; }}")
         L.append(f"  static __device__ __forceinline__ const unsigned short* outs() {{ return k_ho_{tag}; }}")
-    if want_wvrr:
+    if want_wvrr and deriv:
         L.append(f"  static __device__ __forceinline__ const unsigned short* vmap() {{ return k_vm_{tag}; }}")
     L.append("  template <class Q, class Sink>")
     L.append("  static __device__ __forceinline__ void vrr(const double* __restrict__ Fp, const Q& q, double wa, double wb,"
@@ -1044,9 +1049,10 @@ def gen_warp_code(cid, la, lb, lc, ld, deriv, p, want_warp=True, want_wvrr=False
         L.append(f"void qx_launch_warp_{tag}(const qx::WarpArgs& w, int mode, cudaStream_t s) "
                  f"{{ qx::launch_warp<Warp_{tag}, {deriv}>(w, mode, s); }}")
     if want_wvrr:
-        L.append(f"void qx_launch_wvrr_{tag}(const qx::EriArgs& a, const int2* tasks, long long ntask, int chunk, "
+        kind = "wvrr" if deriv else "pvrr"
+        L.append(f"void qx_launch_{kind}_{tag}(const qx::EriArgs& a, const int2* tasks, long long ntask, int chunk, "
                  f"double* acc, int nacc, cudaStream_t s) "
-                 f"{{ qx::launch_wvrr<Warp_{tag}>(a, tasks, ntask, chunk, acc, nacc, s); }}")
+                 f"{{ qx::launch_gvrr<Warp_{tag}, {'true' if deriv else 'false'}>(a, tasks, ntask, chunk, acc, nacc, s); }}")
     return "\n".join(L)
 
 
@@ -1098,11 +1104,13 @@ def main():
     for fn in os.listdir(os.path.join(here, "gen")):
         if fn.startswith("k_eri_") and fn.endswith(".cu"):
             os.remove(os.path.join(here, "gen", fn))
-    wp, wd, wh, wv = [], [], [], []
+    wp, wd, wh, wv, wq = [], [], [], [], []
     for i, (a, b, c, d) in enumerate(qc):
         okp, pp = warp_feasible(a, b, c, d, 0)
         okd, pd = warp_feasible(a, b, c, d, 1)
         okv = wvrr_wanted(a, b, c, d) and pd["peak"] <= WARP_PEAK_MAX
+        okq = okp and pvrr_wanted(a, b, c, d)
+        wq.append(okq)
         okh = max(a, b, c, d) <= 1
         ph = warp_program(a, b, c, d, 2) if okh else None
         wp.append(okp)
@@ -1119,7 +1127,7 @@ def main():
             if (a, b, c, d) not in COOP_CLASSES:
                 f.write(f"QX_DEFINE_LAUNCH({i}, {a}, {b}, {c}, {d})\n")
             if okp:
-                f.write(gen_warp_code(i, a, b, c, d, 0, pp) + "\n")
+                f.write(gen_warp_code(i, a, b, c, d, 0, pp, want_wvrr=okq) + "\n")
             if okd or okv:
                 f.write(gen_warp_code(i, a, b, c, d, 1, pd, want_warp=okd, want_wvrr=okv) + "\n")
             if okh:
@@ -1131,6 +1139,8 @@ def main():
         f.write("#define QX_FOR_EACH_WARP_PLAIN(X) " + " ".join(f"X({i:02d})" for i, x in enumerate(wp) if x) + "\n")
         f.write("#define QX_FOR_EACH_WARP_DERIV(X) " + " ".join(f"X({i:02d})" for i, x in enumerate(wd) if x) + "\n")
         f.write("#define QX_CLASS_WVRR {" + ", ".join("1" if x else "0" for x in wv) + "}\n")
+        f.write("#define QX_CLASS_PVRR {" + ", ".join("1" if x else "0" for x in wq) + "}\n")
+        f.write("#define QX_FOR_EACH_PVRR(X) " + " ".join(f"X({i:02d})" for i, x in enumerate(wq) if x) + "\n")
         f.write("#define QX_FOR_EACH_WVRR(X) " + " ".join(f"X({i:02d})" for i, x in enumerate(wv) if x) + "\n")
         f.write("#define QX_CLASS_WARP_DERIV2 {" + ", ".join("1" if x else "0" for x in wh) + "}\n")
         f.write("#define QX_FOR_EACH_WARP_DERIV2(X) " + " ".join(f"X({i:02d})" for i, x in enumerate(wh) if x) + "\n")

@@ -93,10 +93,12 @@ static const int g_class_nacc[QX_NUM_CLASSES] = QX_CLASS_NACC;
 static const int g_has_warp_plain[QX_NUM_CLASSES] = QX_CLASS_WARP_PLAIN;
 static const int g_has_warp_deriv[QX_NUM_CLASSES] = QX_CLASS_WARP_DERIV;
 static const int g_has_wvrr[QX_NUM_CLASSES] = QX_CLASS_WVRR;
+static const int g_has_pvrr[QX_NUM_CLASSES] = QX_CLASS_PVRR;
 static WarpLaunch g_warp_plain[QX_NUM_CLASSES];
 static WarpLaunch g_warp_deriv[QX_NUM_CLASSES];
 static WarpLaunch g_warp_deriv2[QX_NUM_CLASSES];  // second derivatives (classes with l <= 1)
 static WvrrLaunch g_wvrr[QX_NUM_CLASSES];          // derivative VRR into global accumulators
+static WvrrLaunch g_pvrr[QX_NUM_CLASSES];          // plain VRR into global accumulators
 #define QX_DECL_WP(id) void qx_launch_warp_p##id(const qx::WarpArgs&, int, cudaStream_t);
 QX_FOR_EACH_WARP_PLAIN(QX_DECL_WP)
 #define QX_DECL_WD(id) void qx_launch_warp_d##id(const qx::WarpArgs&, int, cudaStream_t);
@@ -106,11 +108,16 @@ QX_FOR_EACH_WARP_DERIV2(QX_DECL_WH)
 #define QX_DECL_WV(id) \
     void qx_launch_wvrr_d##id(const qx::EriArgs&, const int2*, long long, int, double*, int, cudaStream_t);
 QX_FOR_EACH_WVRR(QX_DECL_WV)
+#define QX_DECL_PV(id) \
+    void qx_launch_pvrr_p##id(const qx::EriArgs&, const int2*, long long, int, double*, int, cudaStream_t);
+QX_FOR_EACH_PVRR(QX_DECL_PV)
 // Engines per class.  Plain ERI: straight-line per-thread kernels (small classes),
 // warp-per-quartet kernels (lanes = primitive quartets), or the cooperative engine
 // (classes whose VRR does not fit a lane's registers).  Derivatives: warp kernels
 // where they fit, else the cooperative derivative engine.
-enum { ENG_SL = 0, ENG_WARP = 1, ENG_COOP = 2, ENG_WVRR = 3 };
+// ENG_WVRR (derivatives): warp-program VRR into global accumulators + the
+// cooperative HRR; ENG_WSPLIT (plain): the same VRR split + the warp HRR.
+enum { ENG_SL = 0, ENG_WARP = 1, ENG_COOP = 2, ENG_WVRR = 3, ENG_WSPLIT = 4 };
 int qx_der_index(int cls);
 void qx_launch_der_split(int der_idx, const qx::EriArgs& a, int mode, const double* D, double cj, double ck,
                          double* grad, int slice, const int2* tasks, long long ntask, double* scratch, cudaStream_t s);
@@ -132,6 +139,7 @@ static bool init_class_tables() {
         g_warp_deriv[c] = nullptr;
         g_warp_deriv2[c] = nullptr;
         g_wvrr[c] = nullptr;
+        g_pvrr[c] = nullptr;
     }
 #define QX_SET_WP(id) g_warp_plain[1##id - 100] = &qx_launch_warp_p##id;
     QX_FOR_EACH_WARP_PLAIN(QX_SET_WP)
@@ -141,6 +149,8 @@ static bool init_class_tables() {
     QX_FOR_EACH_WARP_DERIV2(QX_SET_WH)
 #define QX_SET_WV(id) g_wvrr[1##id - 100] = &qx_launch_wvrr_d##id;
     QX_FOR_EACH_WVRR(QX_SET_WV)
+#define QX_SET_PV(id) g_pvrr[1##id - 100] = &qx_launch_pvrr_p##id;
+    QX_FOR_EACH_PVRR(QX_SET_PV)
 #define QX_SL_ENTRY(id, a, b, c, d)                            \
     g_eri_launch[id] = &qx_launch_eri_##id;                    \
     g_class_scratch[id] = qx::scratch_per_quartet<a, b, c, d>();
@@ -199,7 +209,14 @@ struct ClassWork {
     int2* d_dtasks = nullptr;
     long long ndtask = 0;
     double* d_dacc = nullptr;
+    // the quartet list is cut into slices whose accumulators fit the split-mode
+    // buffers; task quartet indices are relative to their slice
+    std::vector<long long> slice_q, slice_t;  // quartet / task boundaries, nslice + 1 each
+    double* d_pacc = nullptr;  // plain split-mode accumulators (one slice)
 };
+
+// Bytes of accumulator buffer the split modes may use per class.
+static constexpr long long QX_SPLIT_ACC_BYTES = 512LL << 20;
 
 static constexpr int QX_NSTREAMS = 8;
 
@@ -244,28 +261,48 @@ struct qx_handle {
     int wpq_deriv[QX_NUM_CLASSES];  // warps per quartet, derivative warp kernels
 };
 
-// Primitive-chunk tasks and accumulator sums of the derivative split mode, built
-// at the first derivative call that needs them.
-static int ensure_deriv_tasks(qx_handle* h, int c) {
+// Primitive-chunk tasks (quartet, first primitive quartet) and the accumulator
+// buffer of the split modes, built at the first call that needs them.  The
+// quartets are cut into slices of at most QX_SPLIT_ACC_BYTES of derivative
+// accumulators; each slice runs as its own VRR + HRR pair.
+static int ensure_split_tasks(qx_handle* h, int c) {
     ClassWork& w = h->work[c];
     if (w.d_dtasks || !w.nq) return QX_OK;
     std::vector<int2> L((size_t)w.nq);
     QX_CUDA(cudaMemcpy(L.data(), w.d_q, sizeof(int2) * w.nq, cudaMemcpyDeviceToHost));
+    const long long nacc = qx_der_nacc(g_der_idx[c]);
+    const long long cap_q = std::max(1LL, QX_SPLIT_ACC_BYTES / (8 * nacc));
     std::vector<int2> tasks;
+    w.slice_q.assign(1, 0);
+    w.slice_t.assign(1, 0);
     const int ch = qx_der_chunk();
-    for (size_t qi = 0; qi < L.size(); ++qi) {
+    long long q0 = 0;
+    for (long long qi = 0; qi < w.nq; ++qi) {
+        if (qi - q0 == cap_q) {
+            q0 = qi;
+            w.slice_q.push_back(qi);
+            w.slice_t.push_back((long long)tasks.size());
+        }
         const int np_q = h->pairs[L[qi].x].nprim * h->pairs[L[qi].y].nprim;
-        for (int t0 = 0; t0 < np_q; t0 += ch) tasks.push_back(make_int2((int)qi, t0));
+        for (int t0 = 0; t0 < np_q; t0 += ch) tasks.push_back(make_int2((int)(qi - q0), t0));
     }
+    w.slice_q.push_back(w.nq);
+    w.slice_t.push_back((long long)tasks.size());
     if (cudaMalloc((void**)&w.d_dtasks, sizeof(int2) * tasks.size()) != cudaSuccess ||
-        cudaMalloc((void**)&w.d_dacc, sizeof(double) * w.nq * qx_der_nacc(g_der_idx[c])) != cudaSuccess) {
+        cudaMalloc((void**)&w.d_dacc, sizeof(double) * std::min(w.nq, cap_q) * nacc) != cudaSuccess) {
         cudaGetLastError();
-        return fail(QX_E_NOMEM, "derivative split-mode buffers for class %d", c);
+        cudaFree(w.d_dtasks);
+        w.d_dtasks = nullptr;
+        return fail(QX_E_NOMEM, "split-mode buffers for class %d", c);
     }
     w.ndtask = (long long)tasks.size();
     QX_CUDA(cudaMemcpy(w.d_dtasks, tasks.data(), sizeof(int2) * tasks.size(), cudaMemcpyHostToDevice));
     return QX_OK;
 }
+
+// Plain items per quartet of the warp programs (the accumulator targets, padded
+// to the 16-item staging groups).
+static long long plain_items(int c) { return (g_class_nacc[c] + 15) / 16 * 16; }
 
 // Warps per quartet: classes with few quartets but long primitive loops let four
 // warps share a quartet so the GPU fills up.
@@ -274,23 +311,29 @@ static int choose_wpq(long long nq, long long prims) {
     return (nq < 20000 && avg >= 4 * 32) ? 4 : 1;
 }
 
-// Default engine choice, overridable with QX_PLAIN_ENGINE=sl|warp|coop and
-// QX_DERIV_ENGINE=warp|coop (for measuring alternatives); an override that a class
+// Default engine choice, overridable with QX_PLAIN_ENGINE=sl|warp|coop|wsplit and
+// QX_DERIV_ENGINE=coop|wvrr (for measuring alternatives); an override that a class
 // cannot honour falls back to the default.
 static void choose_engines(qx_handle* h) {
     const char* pe = std::getenv("QX_PLAIN_ENGINE");
     const char* de = std::getenv("QX_DERIV_ENGINE");
     for (int c = 0; c < QX_NUM_CLASSES; ++c) {
         int p;
-        if (g_has_warp_plain[c] && g_class_nacc[c] > 48) p = ENG_WARP;
+        if (g_has_pvrr[c]) p = ENG_WSPLIT;  // measured fastest for these classes
+        else if (g_has_warp_plain[c] && g_class_nacc[c] > 48) p = ENG_WARP;
         else if (!g_class_coop[c]) p = ENG_SL;
         else p = g_has_warp_plain[c] ? ENG_WARP : ENG_COOP;
         if (pe) {
             if (!std::strcmp(pe, "sl") && !g_class_coop[c]) p = ENG_SL;
             if (!std::strcmp(pe, "warp") && g_has_warp_plain[c]) p = ENG_WARP;
             if (!std::strcmp(pe, "coop") && g_class_coop[c]) p = ENG_COOP;
+            if (!std::strcmp(pe, "wsplit") && g_has_pvrr[c]) p = ENG_WSPLIT;
         }
-        int d = g_has_warp_deriv[c] ? ENG_WARP : (g_has_wvrr[c] ? ENG_WVRR : ENG_COOP);
+        // the global-accumulator VRR wins for the classes with L >= 6 (measured);
+        // the autotuner settles the rest per molecule
+        const int L = g_class_l[c][0] + g_class_l[c][1] + g_class_l[c][2] + g_class_l[c][3];
+        int d = (g_has_wvrr[c] && (L >= 6 || !g_has_warp_deriv[c])) ? ENG_WVRR
+                : (g_has_warp_deriv[c] ? ENG_WARP : ENG_COOP);
         if (de && !std::strcmp(de, "coop")) d = ENG_COOP;
         if (de && !std::strcmp(de, "wvrr") && g_has_wvrr[c]) d = ENG_WVRR;
         h->plain_eng[c] = p;
@@ -312,6 +355,7 @@ static void free_handle(qx_handle* h) {
         cudaFree(w.scratch);
         cudaFree(w.d_dtasks);
         cudaFree(w.d_dacc);
+        cudaFree(w.d_pacc);
     }
     for (int i = 0; i < QX_NSTREAMS; ++i) {
         if (h->streams[i]) cudaStreamDestroy(h->streams[i]);
@@ -347,7 +391,7 @@ static int run_class(qx_handle* h, int cls, int mode, const int2* d_q, long long
     a.err = h->d_err;
     if (eng == ENG_COOP) {
         qx_launch_coop(g_coop_idx[cls], a, mode, s);
-    } else if (eng == ENG_WARP) {
+    } else if (eng == ENG_WARP || eng == ENG_WSPLIT) {
         WarpArgs wa;
         wa.e = a;
         wa.wpq = h->wpq[cls];
@@ -355,6 +399,22 @@ static int run_class(qx_handle* h, int cls, int mode, const int2* d_q, long long
         wa.cj = wa.ck = 0.0;
         wa.grad = nullptr;
         wa.slice = -1;
+        ClassWork& w = h->work[cls];
+        if (eng == ENG_WSPLIT && d_q == w.d_q && !ensure_split_tasks(h, cls) && w.slice_q.size() == 2) {
+            // VRR by (quartet, primitive chunk) tasks into global accumulators, then
+            // the warp HRR + epilogue from them (one quartet per warp).  A class too
+            // large for one accumulator slice runs the plain warp kernel instead.
+            const long long np = plain_items(cls);
+            if (!w.d_pacc && cudaMalloc((void**)&w.d_pacc, sizeof(double) * w.nq * np) != cudaSuccess) {
+                cudaGetLastError();
+                w.d_pacc = nullptr;
+                return fail(QX_E_NOMEM, "plain split-mode accumulators for class %d", cls);
+            }
+            QX_CUDA(cudaMemsetAsync(w.d_pacc, 0, sizeof(double) * w.nq * np, s));
+            g_pvrr[cls](a, w.d_dtasks, w.ndtask, qx_der_chunk(), w.d_pacc, (int)np, s);
+            wa.wpq = 1;
+            wa.acc_in = w.d_pacc;
+        }
         g_warp_plain[cls](wa, mode, s);
     } else {
         g_eri_launch[cls](a, mode, s);
@@ -727,23 +787,28 @@ static int run_deriv_class(qx_handle* h, int c, int mode, double* out, const dou
         wa.grad = grad;
         wa.slice = slice;
         g_warp_deriv[c](wa, mode, cs);
-    } else if (h->deriv_eng[c] == ENG_WVRR) {
-        // warp-program VRR into global accumulators, then the cooperative HRR pass
-        int rc = ensure_deriv_tasks(h, c);
+    } else {
+        // split modes, slice by slice: warp-program VRR into global accumulators
+        // (ENG_WVRR) or the cooperative VRR, then the cooperative HRR pass
+        if (g_der_idx[c] < 0) return fail(QX_E_UNSUPPORTED, "no derivative program for class %d", c);
+        int rc = ensure_split_tasks(h, c);
         if (rc) return rc;
         const ClassWork& w = h->work[c];
         const long long nacc = qx_der_nacc(g_der_idx[c]);
-        QX_CUDA(cudaMemsetAsync(w.d_dacc, 0, sizeof(double) * w.nq * nacc, cs));
-        const EriArgs a = class_args(h, c, out);
-        g_wvrr[c](a, w.d_dtasks, w.ndtask, qx_der_chunk(), w.d_dacc, (int)nacc, cs);
-        qx_launch_der_hrr(g_der_idx[c], a, mode, D, cj, ck, grad, slice, w.d_dacc, cs);
-    } else {
-        if (g_der_idx[c] < 0) return fail(QX_E_UNSUPPORTED, "no derivative program for class %d", c);
-        int rc = ensure_deriv_tasks(h, c);
-        if (rc) return rc;
-        const ClassWork& w = h->work[c];
-        qx_launch_der_split(g_der_idx[c], class_args(h, c, out), mode, D, cj, ck, grad, slice, w.d_dtasks,
-                            w.ndtask, w.d_dacc, cs);
+        for (size_t sl = 0; sl + 1 < w.slice_q.size(); ++sl) {
+            EriArgs a = class_args(h, c, out);
+            a.quartets = w.d_q + w.slice_q[sl];
+            a.nq = w.slice_q[sl + 1] - w.slice_q[sl];
+            const int2* tk = w.d_dtasks + w.slice_t[sl];
+            const long long nt = w.slice_t[sl + 1] - w.slice_t[sl];
+            if (h->deriv_eng[c] == ENG_WVRR) {
+                QX_CUDA(cudaMemsetAsync(w.d_dacc, 0, sizeof(double) * a.nq * nacc, cs));
+                g_wvrr[c](a, tk, nt, qx_der_chunk(), w.d_dacc, (int)nacc, cs);
+                qx_launch_der_hrr(g_der_idx[c], a, mode, D, cj, ck, grad, slice, w.d_dacc, cs);
+            } else {
+                qx_launch_der_split(g_der_idx[c], a, mode, D, cj, ck, grad, slice, tk, nt, w.d_dacc, cs);
+            }
+        }
     }
     QX_CUDA(cudaGetLastError());
     return QX_OK;
@@ -998,12 +1063,14 @@ extern "C" int qx_autotune(qx_handle* h, int what, void* stream) {
                 cand.push_back({ENG_WARP, 4});
             }
             if (g_class_coop[c]) cand.push_back({ENG_COOP, 0});
+            if (g_has_pvrr[c] && g_has_warp_plain[c] && !ensure_split_tasks(h, c) && w.slice_q.size() == 2)
+                cand.push_back({ENG_WSPLIT, 1});
             const int keep_wpq = h->wpq[c], keep_lg = w.log2g;
             float best = 1e30f;
             TuneCfg bc{h->plain_eng[c], h->plain_eng[c] == ENG_SL ? keep_lg : keep_wpq};
             for (const TuneCfg& t : cand) {
                 h->plain_eng[c] = t.eng;
-                if (t.eng == ENG_WARP) h->wpq[c] = t.param;
+                if (t.eng == ENG_WARP || t.eng == ENG_WSPLIT) h->wpq[c] = t.param;
                 const int lg = t.eng == ENG_SL ? t.param : 0;
                 float ms = 0.f;
                 rc = time_config(s, e0, e1, &ms, [&] {
@@ -1016,7 +1083,7 @@ extern "C" int qx_autotune(qx_handle* h, int what, void* stream) {
                 }
             }
             h->plain_eng[c] = bc.eng;
-            h->wpq[c] = bc.eng == ENG_WARP ? bc.param : keep_wpq;
+            h->wpq[c] = (bc.eng == ENG_WARP || bc.eng == ENG_WSPLIT) ? bc.param : keep_wpq;
             w.log2g = bc.eng == ENG_SL ? bc.param : keep_lg;
         }
         if ((what & 2) && !rc) {

@@ -23,6 +23,9 @@ struct WarpArgs {
     double cj, ck;
     double* grad;  // adjoint: 3N
     int slice;     // single derivative slice
+    // split mode: the quartets' accumulators (NITEM_PAD per quartet, item order)
+    // were summed by k_gvrr; the kernel runs only the HRR and the epilogue
+    const double* acc_in = nullptr;
 };
 
 enum { WMODE_DENSE = 0, WMODE_UNIQUE = 1, WMODE_SCHWARZ = 2, WMODE_DER_DENSE = 10, WMODE_DER_SLICE = 11,
@@ -75,6 +78,14 @@ struct SmemSink {
     double* acc;
     __device__ __forceinline__ void operator()(double (&v)[16], int base, unsigned lane) const {
         reduce16(v, acc + base, lane);
+    }
+};
+
+struct IdentSink {
+    double* acc;
+    __device__ __forceinline__ void operator()(double (&v)[16], int base, unsigned lane) const {
+        reduce16_core(v, lane);
+        if (!(lane & 1)) atomicAdd(acc + base + (lane >> 1), v[0]);
     }
 };
 
@@ -204,9 +215,14 @@ __global__ void __launch_bounds__(WARP_QPB * 32) k_warp(WarpArgs wa, int mode) {
                 return;
         }
     }
-    for (int t = lane; t < W::NITEM_PAD; t += 32) H[t] = 0.0;
+    if (wa.acc_in) {
+        const double* __restrict__ src = wa.acc_in + (size_t)qi * W::NITEM_PAD;
+        for (int t = lane; t < W::NITEM_PAD; t += 32) H[t] = src[t];
+    } else {
+        for (int t = lane; t < W::NITEM_PAD; t += 32) H[t] = 0.0;
+    }
     __syncwarp();
-    const int nk = Q.nprim, ntot = P.nprim * nk;
+    const int nk = Q.nprim, ntot = wa.acc_in ? 0 : P.nprim * nk;
     for (int t0 = 32 * sub; t0 < ntot; t0 += 32 * wpq) {
         const int t = t0 + (int)lane;
         const bool act = t < ntot;
@@ -378,13 +394,16 @@ void launch_warp(const WarpArgs& wa, int mode, cudaStream_t s) {
 
 typedef void (*WarpLaunch)(const WarpArgs&, int mode, cudaStream_t);
 
-// Derivative VRR of one (quartet, primitive chunk) task per warp into the
-// quartet's global accumulators (cooperative derivative layout), which the
-// cooperative HRR pass then turns into integrals.  For the largest classes, whose
-// accumulators and HRR slots do not fit a warp's shared memory.  acc must be
-// zeroed before the launch.
-template <class W>
-__global__ void __launch_bounds__(WARP_QPB * 32) k_wvrr(EriArgs a, const int2* __restrict__ tasks, long long ntask,
+// VRR of one (quartet, primitive chunk) task per warp into the quartet's global
+// accumulators; another kernel then runs the HRR from them.  For the classes with
+// few quartets and long primitive loops (many warps per quartet keep the GPU
+// full) and for the derivative classes whose accumulators and HRR slots do not
+// fit a warp's shared memory.  Derivative programs (DER) map items to the
+// cooperative engine's accumulator layout (nacc per quartet); plain programs keep
+// the item order (NITEM_PAD per quartet).  Task quartet indices are relative to
+// a.quartets; acc must be zeroed before the launch.
+template <class W, bool DER>
+__global__ void __launch_bounds__(WARP_QPB * 32) k_gvrr(EriArgs a, const int2* __restrict__ tasks, long long ntask,
                                                          int chunk, double* __restrict__ acc, int nacc) {
     const unsigned lane = threadIdx.x & 31;
     const long long ti = (long long)blockIdx.x * WARP_QPB + (threadIdx.x >> 5);
@@ -393,8 +412,8 @@ __global__ void __launch_bounds__(WARP_QPB * 32) k_wvrr(EriArgs a, const int2* _
     const int2 pq = a.quartets[task.x];
     const PairInfo P = a.pairs[pq.x];
     const PairInfo Q = a.pairs[pq.y];
-    if (P.atom1 == P.atom2 && P.atom1 == Q.atom1 && P.atom1 == Q.atom2) return;  // reference skips these
-    const GlobalSink sink{acc + (size_t)task.x * nacc, W::vmap()};
+    if (DER && P.atom1 == P.atom2 && P.atom1 == Q.atom1 && P.atom1 == Q.atom2) return;  // reference skips these
+    double* qacc = acc + (size_t)task.x * (DER ? nacc : W::NITEM_PAD);
     extern __shared__ double wv_sm[];
     double* save = wv_sm + (size_t)(threadIdx.x >> 5) * W::SAVE;
     const int nk = Q.nprim, ntot = P.nprim * nk;
@@ -413,18 +432,23 @@ __global__ void __launch_bounds__(WARP_QPB * 32) k_wvrr(EriArgs a, const int2* _
 #pragma unroll
             for (int m = 0; m <= W::S; ++m) Fp[m] = 0.0;
         }
-        W::vrr(Fp, q, 2.0 * p.alpha, 2.0 * (p.zeta - p.alpha), 2.0 * r.alpha, sink, lane, save);
+        const double wa = 2.0 * p.alpha, wb = 2.0 * (p.zeta - p.alpha), wc = 2.0 * r.alpha;
+        if constexpr (DER)
+            W::vrr(Fp, q, wa, wb, wc, GlobalSink{qacc, W::vmap()}, lane, save);
+        else
+            W::vrr(Fp, q, wa, wb, wc, IdentSink{qacc}, lane, save);
         __syncwarp();
     }
 }
 
-template <class W>
-void launch_wvrr(const EriArgs& a, const int2* tasks, long long ntask, int chunk, double* acc, int nacc,
+template <class W, bool DER>
+void launch_gvrr(const EriArgs& a, const int2* tasks, long long ntask, int chunk, double* acc, int nacc,
                  cudaStream_t s) {
     const long long nb = (ntask + WARP_QPB - 1) / WARP_QPB;
     const size_t smem = sizeof(double) * (size_t)W::SAVE * WARP_QPB;
-    if (smem > 48 * 1024) cudaFuncSetAttribute(k_wvrr<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (nb) k_wvrr<W><<<(unsigned)nb, WARP_QPB * 32, smem, s>>>(a, tasks, ntask, chunk, acc, nacc);
+    auto k = k_gvrr<W, DER>;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (nb) k<<<(unsigned)nb, WARP_QPB * 32, smem, s>>>(a, tasks, ntask, chunk, acc, nacc);
 }
 
 typedef void (*WvrrLaunch)(const EriArgs&, const int2*, long long, int, double*, int, cudaStream_t);

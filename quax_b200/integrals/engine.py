@@ -141,7 +141,7 @@ class EriEngine:
             )
         return out
 
-    ENGINE_NAMES = ("sl", "warp", "coop", "wvrr")
+    ENGINE_NAMES = ("sl", "warp", "coop", "wvrr", "wsplit")
 
     def autotune(self, plain: bool = True, deriv: bool = True, stream=None) -> None:
         """Time every engine configuration per class on this molecule and keep the fastest."""
