@@ -176,6 +176,8 @@ def run_ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
+    if args.no_extras:
+        torch.cuda.profiler.start()  # profiling runs: the steps only (ncu --profile-from-start off)
     for _ in range(args.warmup):
         eng.eri_unique(out)
     barrier()
@@ -199,6 +201,7 @@ def run_ours(args):
     launches = sum(1 for c in info if c["nq"] > 0) * args.steps
 
     if args.no_extras:
+        torch.cuda.profiler.stop()
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": "quartets/s", "ms_per_step": ms_per_step,
                               "note": "--no-extras (profiling run)"}), flush=True)
@@ -234,7 +237,10 @@ def run_ours(args):
         "unit": "TFLOP/s",
         "frac": achieved / peak if peak > 0 else None,
         "peak_source": "measured FP64 FMA probe (libqx_peaks.so), not in MEASURED_PEAKS.json",
-        "traffic": None,
+        # DRAM bytes per launch of the dominant kernel from one ncu capture
+        # (profiles/k_gvrr_p19_eri10.md); null when another class dominates
+        "traffic": 29.21e6 if tuple(dom["l"]) == (2, 2, 2, 1) else None,
+        "traffic_unit": "bytes per launch (VRR split kernel of the class, ncu)",
         "step_achieved_tflops": total_flops / (ms_per_step * 1e-3) / 1e12,
         "dominant_share_of_serial_sum": dom_ms / sum(p[0] for p in per),
     }
