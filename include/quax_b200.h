@@ -150,6 +150,18 @@ int qx_eri_unique_class(qx_handle *h, int cls, double *out_dev, void *stream);
 int qx_grad_adjoint_class(qx_handle *h, int cls, const double *D_dev, double cj, double ck, double *grad_dev,
                           void *stream);
 
+/* Multi-GPU sharding, no counterpart in the reference (which runs on one host).
+ * qx_set_shard restricts the handle to rank `rank` of `nranks`: each class keeps a
+ * cost-balanced contiguous range of its screened quartets, so per-rank results
+ * (dense and derivative tensors, J, K, adjoint gradients) sum over the ranks to
+ * the full result -- one all-reduce.  The unique layout and qx_unique_quartets
+ * then describe this rank's quartets.  Synchronises the device; call it before
+ * qx_autotune.  nranks = 1 restores the full lists.
+ * qx_partition_costs is the host-only cut it uses: items with costs cost[0..n)
+ * split into nranks contiguous ranges bounds[r]..bounds[r+1] of near-equal cost. */
+int qx_set_shard(qx_handle *h, int rank, int nranks);
+int qx_partition_costs(const double *cost, long long n, int nranks, long long *bounds);
+
 /* Autotuner, no counterpart in the reference.  Times, on this handle's own
  * quartet lists, every engine configuration each class can run and keeps the
  * fastest: straight-line kernels with 1..32 lanes per quartet, warp kernels with

@@ -199,7 +199,9 @@ static void boys_table_host(std::vector<double>& tab) {
 // ------------------------------------------------------------------ handle ----
 struct ClassWork {
     long long nq = 0;
-    int2* d_q = nullptr;
+    int2* d_q = nullptr;       // this rank's quartets: a view into d_q_full
+    int2* d_q_full = nullptr;  // the class's full screened list (owned)
+    long long nq_full = 0;
     long long unique_base = 0;
     long long prims = 0;       // primitive quartets of the class
     int log2g = 0;             // lanes per quartet = 2^log2g
@@ -351,7 +353,7 @@ static void free_handle(qx_handle* h) {
     cudaFree(h->d_err);
     cudaFree(h->d_scratch);
     for (auto& w : h->work) {
-        cudaFree(w.d_q);
+        cudaFree(w.d_q_full);
         cudaFree(w.scratch);
         cudaFree(w.d_dtasks);
         cudaFree(w.d_dacc);
@@ -637,6 +639,8 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
         if (w.nq) {
             QX_ALLOC(w.d_q, sizeof(int2) * w.nq);
             cudaMemcpy(w.d_q, sorted.data(), sizeof(int2) * w.nq, cudaMemcpyHostToDevice);
+            w.d_q_full = w.d_q;
+            w.nq_full = w.nq;
             if (g_class_scratch[c] && h->plain_eng[c] == ENG_SL)
                 QX_ALLOC(w.scratch, sizeof(double) * g_class_scratch[c] * launch_threads(w.nq, w.log2g));
         }
@@ -663,6 +667,80 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
         return fail(QX_E_CUDA, "qx_initialize: %s", cudaGetErrorString(e));
     }
     *out = h;
+    return QX_OK;
+}
+
+// ------------------------------------------------------------------ shards ----
+// Cost-balanced contiguous cut of a list: item i (cost c_i, prefix C_i, total T)
+// goes to rank floor(nranks (C_i + c_i / 2) / T), which is monotone in i, so each
+// rank gets one contiguous range; bounds[r] .. bounds[r+1] is rank r's.
+extern "C" int qx_partition_costs(const double* cost, long long n, int nranks, long long* bounds) {
+    if (!bounds || nranks < 1 || n < 0 || (n > 0 && !cost)) return fail(QX_E_INVALID, "qx_partition_costs: bad argument");
+    double T = 0.0;
+    for (long long i = 0; i < n; ++i) {
+        if (!(cost[i] >= 0.0) || !std::isfinite(cost[i])) return fail(QX_E_INVALID, "qx_partition_costs: bad cost");
+        T += cost[i];
+    }
+    for (int r = 0; r <= nranks; ++r) bounds[r] = r == 0 ? 0 : n;
+    if (n == 0) return QX_OK;
+    double C = 0.0;
+    int cur = 0;
+    for (long long i = 0; i < n; ++i) {
+        int r = T > 0.0 ? (int)std::floor(nranks * (C + 0.5 * cost[i]) / T) : (int)(i * nranks / n);
+        r = std::min(std::max(r, cur), nranks - 1);
+        while (cur < r) bounds[++cur] = i;
+        C += cost[i];
+    }
+    while (cur < nranks - 1) bounds[++cur] = n;
+    bounds[nranks] = n;
+    return QX_OK;
+}
+
+// Restrict the handle to rank `rank` of `nranks`: every class keeps a
+// cost-balanced contiguous range of its screened quartets (cost = primitive
+// quartets), so the ranks' results (dense tensors, derivative tensors, J, K,
+// gradients) sum to the full one.  The unique layout then holds this rank's
+// quartets only.  nranks = 1 restores the full lists.
+extern "C" int qx_set_shard(qx_handle* h, int rank, int nranks) {
+    if (!h || nranks < 1 || rank < 0 || rank >= nranks) return fail(QX_E_INVALID, "qx_set_shard: bad rank/nranks");
+    DeviceGuard g(h->device);
+    QX_CUDA(cudaDeviceSynchronize());
+    long long base = 0;
+    h->nunique = 0;
+    for (int c = 0; c < QX_NUM_CLASSES; ++c) {
+        ClassWork& w = h->work[c];
+        // split-mode buffers belong to the old range
+        cudaFree(w.d_dtasks);
+        cudaFree(w.d_dacc);
+        cudaFree(w.d_pacc);
+        w.d_dtasks = nullptr;
+        w.d_dacc = w.d_pacc = nullptr;
+        w.ndtask = 0;
+        w.slice_q.clear();
+        w.slice_t.clear();
+        long long lo = 0, hi = w.nq_full;
+        long long prims = 0;
+        if (w.nq_full) {
+            std::vector<int2> L((size_t)w.nq_full);
+            QX_CUDA(cudaMemcpy(L.data(), w.d_q_full, sizeof(int2) * w.nq_full, cudaMemcpyDeviceToHost));
+            std::vector<double> cost((size_t)w.nq_full);
+            for (long long i = 0; i < w.nq_full; ++i)
+                cost[i] = (double)h->pairs[L[i].x].nprim * h->pairs[L[i].y].nprim;
+            std::vector<long long> b(nranks + 1);
+            int rc = qx_partition_costs(cost.data(), w.nq_full, nranks, b.data());
+            if (rc) return rc;
+            lo = b[rank];
+            hi = b[rank + 1];
+            for (long long i = lo; i < hi; ++i) prims += (long long)cost[i];
+        }
+        w.d_q = w.d_q_full + lo;
+        w.nq = hi - lo;
+        w.prims = prims;
+        w.unique_base = base;
+        base += w.nq * g_class_nout[c];
+        h->nunique += w.nq;
+    }
+    h->unique_size = base;
     return QX_OK;
 }
 

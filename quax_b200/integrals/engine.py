@@ -70,6 +70,12 @@ class EriEngine:
         return self._h
 
     # -- queries --------------------------------------------------------------
+    def set_shard(self, rank: int, nranks: int) -> None:
+        """Keep a cost-balanced contiguous range of every class's quartets (rank of
+        nranks); results of the ranks then sum to the full ones."""
+        with torch.cuda.device(self.device):
+            _lib.check(_lib.load().qx_set_shard(self.handle, int(rank), int(nranks)), "qx_set_shard")
+
     def unique_quartets(self) -> int:
         return int(_lib.load().qx_unique_quartets(self.handle))
 
