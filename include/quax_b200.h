@@ -141,6 +141,15 @@ int qx_num_classes(void);
 int qx_class_info(const qx_handle *h, int cls, int *l4, long long *nquartets, long long *nprim_quartets,
                   double *flops, double *flops_deriv);
 
+/* Hessian-vector product of the adjoint, no counterpart in the reference (which
+ * forms Hessians by jacfwd through eri_deriv_jvp, tei.py:342-346, over the order-2
+ * tensor): Hv = sum_nu2 v_nu2 sum_ijkl Gamma_ijkl d2(ij|kl)/dR_nu1 dR_nu2 with
+ * Gamma fixed (as in qx_grad_adjoint), one Hessian column per call for a unit v,
+ * without the 3N(3N+1)/2 * n^4 tensor.  v and Hv hold 3N doubles.  This build:
+ * s and p shells (QX_E_UNSUPPORTED otherwise). */
+int qx_grad_adjoint_jvp(qx_handle *h, const double *D, double cj, double ck, const double *v, double *Hv,
+                        int on_device, void *stream);
+
 /* qx_eri_unique restricted to one class (same output positions). */
 int qx_eri_unique_class(qx_handle *h, int cls, double *out_dev, void *stream);
 

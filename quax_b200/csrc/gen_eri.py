@@ -988,7 +988,7 @@ def warp_save(p):
 
 
 def warp_smem(p, deriv):
-    return p["hslots"] + 32 + (p["nout"] if deriv == 1 else 0) + warp_save(p)
+    return p["hslots"] + 32 + (p["nout"] if deriv in (1, 2) else 0) + warp_save(p)
 
 
 def gen_warp_code(cid, la, lb, lc, ld, deriv, p, want_warp=True, want_wvrr=False):

@@ -128,7 +128,7 @@ void qx_launch_der_hrr(int der_idx, const qx::EriArgs& a, int mode, const double
 void qx_launch_der(int der_idx, const qx::EriArgs& a, int mode, const double* D, double cj, double ck, double* grad,
                    int slice, cudaStream_t s);
 enum { QX_MODE_DER_DENSE = 10, QX_MODE_DER_SLICE = 11, QX_MODE_GRAD = 12, QX_MODE_DER2_DENSE = 13,
-       QX_MODE_DER2_SLICE = 14 };
+       QX_MODE_DER2_SLICE = 14, QX_MODE_HVP = 15 };
 static bool init_class_tables() {
     for (int c = 0; c < QX_NUM_CLASSES; ++c) {
         g_eri_launch[c] = nullptr;
@@ -914,7 +914,8 @@ static int run_all_deriv(qx_handle* h, int mode, double* out, const double* D, d
 
 // Second derivatives: every class through its warp order-2 program.  `slice` is
 // 3N for the dense tensor, or the packed nuclear pair nu1 | nu2 << 16 (nu1 <= nu2).
-static int run_all_deriv2(qx_handle* h, int mode, double* out, int slice, cudaStream_t s) {
+static int run_all_deriv2(qx_handle* h, int mode, double* out, int slice, cudaStream_t s, const double* D = nullptr,
+                          double cj = 0.0, double ck = 0.0, double* hv = nullptr, const double* dir = nullptr) {
     for (int c = 0; c < QX_NUM_CLASSES; ++c)
         if (h->work[c].nq && !g_warp_deriv2[c])
             return fail(QX_E_UNSUPPORTED,
@@ -930,10 +931,12 @@ static int run_all_deriv2(qx_handle* h, int mode, double* out, int slice, cudaSt
         WarpArgs wa;
         wa.e = class_args(h, c, out);
         wa.wpq = h->wpq_deriv[c];
-        wa.D = nullptr;
-        wa.cj = wa.ck = 0.0;
-        wa.grad = nullptr;
+        wa.D = D;
+        wa.cj = cj;
+        wa.ck = ck;
+        wa.grad = hv;
         wa.slice = slice;
+        wa.dir = dir;
         g_warp_deriv2[c](wa, mode, cs);
         QX_CUDA(cudaGetLastError());
     }
@@ -1036,6 +1039,46 @@ extern "C" int qx_grad_adjoint(qx_handle* h, const double* D, double cj, double 
     }
     cudaFree(dD);
     cudaFree(dg);
+    if (!rc) rc = check_err_word(h, s);
+    return rc;
+}
+
+extern "C" int qx_grad_adjoint_jvp(qx_handle* h, const double* D, double cj, double ck, const double* v, double* Hv,
+                                   int on_device, void* stream) {
+    if (!h || !D || !v || !Hv) return fail(QX_E_INVALID, "qx_grad_adjoint_jvp: NULL argument");
+    if (!std::isfinite(cj) || !std::isfinite(ck))
+        return fail(QX_E_INVALID, "qx_grad_adjoint_jvp: non-finite coefficient");
+    DeviceGuard g(h->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const long long n = h->nbf;
+    const int N3 = 3 * h->natom;
+    if (on_device) {
+        QX_CUDA(cudaMemsetAsync(Hv, 0, sizeof(double) * N3, s));
+        return run_all_deriv2(h, QX_MODE_HVP, nullptr, -1, s, D, cj, ck, Hv, v);
+    }
+    double *dD = nullptr, *dv = nullptr, *dh = nullptr;
+    if (cudaMalloc((void**)&dD, sizeof(double) * n * n) != cudaSuccess ||
+        cudaMalloc((void**)&dv, sizeof(double) * N3) != cudaSuccess ||
+        cudaMalloc((void**)&dh, sizeof(double) * N3) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(dD);
+        cudaFree(dv);
+        return fail(QX_E_NOMEM, "qx_grad_adjoint_jvp: staging allocation failed");
+    }
+    int rc = QX_OK;
+    cudaError_t e = cudaMemcpyAsync(dD, D, sizeof(double) * n * n, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dv, v, sizeof(double) * N3, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dh, 0, sizeof(double) * N3, s);
+    if (e != cudaSuccess) rc = fail(QX_E_CUDA, "qx_grad_adjoint_jvp: %s", cudaGetErrorString(e));
+    if (!rc) rc = run_all_deriv2(h, QX_MODE_HVP, nullptr, -1, s, dD, cj, ck, dh, dv);
+    if (!rc) {
+        e = cudaMemcpyAsync(Hv, dh, sizeof(double) * N3, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) rc = fail(QX_E_CUDA, "qx_grad_adjoint_jvp: %s", cudaGetErrorString(e));
+    }
+    cudaFree(dD);
+    cudaFree(dv);
+    cudaFree(dh);
     if (!rc) rc = check_err_word(h, s);
     return rc;
 }

@@ -23,13 +23,14 @@ struct WarpArgs {
     double cj, ck;
     double* grad;  // adjoint: 3N
     int slice;     // single derivative slice
+    const double* dir = nullptr;  // Hessian-vector product: direction (3N)
     // split mode: the quartets' accumulators (NITEM_PAD per quartet, item order)
     // were summed by k_gvrr; the kernel runs only the HRR and the epilogue
     const double* acc_in = nullptr;
 };
 
 enum { WMODE_DENSE = 0, WMODE_UNIQUE = 1, WMODE_SCHWARZ = 2, WMODE_DER_DENSE = 10, WMODE_DER_SLICE = 11,
-       WMODE_GRAD = 12, WMODE_DER2_DENSE = 13, WMODE_DER2_SLICE = 14 };
+       WMODE_GRAD = 12, WMODE_DER2_DENSE = 13, WMODE_DER2_SLICE = 14, WMODE_HVP = 15 };
 
 constexpr int WARP_QPB = 4;  // quartets (warps) per block
 
@@ -260,7 +261,7 @@ __global__ void __launch_bounds__(WARP_QPB * 32) k_warp(WarpArgs wa, int mode) {
     constexpr int NB = ncart_h(W::LB), NC = ncart_h(W::LC), ND = ncart_h(W::LD);
     const bool s12 = P.s1 != P.s2, s34 = Q.s1 != Q.s2, sPQ = pq.x != pq.y;
     const long long n = a.n;
-    if (DERIV == 1 && mode == WMODE_GRAD) {
+    if ((DERIV == 1 && mode == WMODE_GRAD) || (DERIV == 2 && mode == WMODE_HVP)) {
         const double* __restrict__ Dm = wa.D;
         const double fJ = (1.0 + sPQ) * (1.0 + s12) * (1.0 + s34), fK = 1.0 + sPQ;
         const double kd = 1.0 + (double)(s12 && s34), kx = (double)s12 + (double)s34;
@@ -296,6 +297,54 @@ __global__ void __launch_bounds__(WARP_QPB * 32) k_warp(WarpArgs wa, int mode) {
             for (int o = lane; o < W::NOUT; o += 32) {
                 const int id = o % ND, ic = (o / ND) % NC, ib = (o / (ND * NC)) % NB, ia = o / (ND * NC * NB);
                 dense_images(a.out, n, P.bf1 + ia, P.bf2 + ib, Q.bf1 + ic, Q.bf2 + id, s12, s34, sPQ, H[__ldg(outs + o)]);
+            }
+        }
+        return;
+    }
+    if (DERIV == 2 && mode == WMODE_HVP) {
+        // Hessian-vector product of E = sum Gamma G with Gamma fixed: along v the
+        // quartet moves by w_X = v(atom X) - v(atom D) for X = A, B, C (D by
+        // invariance), so sum_V w_V h[U,V] is the directional derivative of the
+        // first-derivative block U; contracted with Gamma it adds to the atom of U
+        // and, with the opposite sign, to the atom of D.
+        double wv[9], h9[9];
+        const int atx[3] = {atA, atB, atC};
+#pragma unroll
+        for (int b = 0; b < 9; ++b) {
+            wv[b] = __ldg(wa.dir + 3 * atx[b / 3] + b % 3) - __ldg(wa.dir + 3 * atD + b % 3);
+            h9[b] = 0.0;
+        }
+        warp_hrr(W::hnodes(), W::hlev(), W::NHLEV, W::outs(), H, geo, lane, [&](int ob, double v) {
+            int pidx = ob / W::NOUT;
+            const int o = ob - pidx * W::NOUT;
+            int Pc = 0;
+            while (pidx >= 9 - Pc) {
+                pidx -= 9 - Pc;
+                ++Pc;
+            }
+            const int Qc = Pc + pidx;
+            const double c = gam[o] * v;
+            double wq = 0.0, wp = 0.0;
+#pragma unroll
+            for (int b = 0; b < 9; ++b) {
+                wq = (b == Qc) ? wv[b] : wq;
+                wp = (b == Pc) ? wv[b] : wp;
+            }
+#pragma unroll
+            for (int b = 0; b < 9; ++b) {
+                h9[b] += (b == Pc) ? c * wq : 0.0;
+                h9[b] += (b == Qc && Pc != Qc) ? c * wp : 0.0;
+            }
+        });
+#pragma unroll
+        for (int b = 0; b < 9; ++b)
+            for (int off = 16; off > 0; off >>= 1) h9[b] += __shfl_xor_sync(0xffffffffu, h9[b], off);
+        if (lane == 0) {
+            for (int x = 0; x < 3; ++x) {
+                atomicAdd(wa.grad + 3 * atA + x, h9[x]);
+                atomicAdd(wa.grad + 3 * atB + x, h9[3 + x]);
+                atomicAdd(wa.grad + 3 * atC + x, h9[6 + x]);
+                atomicAdd(wa.grad + 3 * atD + x, -(h9[x] + h9[3 + x] + h9[6 + x]));
             }
         }
         return;

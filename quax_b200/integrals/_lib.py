@@ -54,6 +54,7 @@ SIGNATURES = {
     "qx_eri_unique_class": (C.c_int, [_vp, C.c_int, _vp, _vp]),
     "qx_grad_adjoint_class": (C.c_int, [_vp, C.c_int, _vp, C.c_double, C.c_double, _vp, _vp]),
     "qx_autotune": (C.c_int, [_vp, C.c_int, _vp]),
+    "qx_grad_adjoint_jvp": (C.c_int, [_vp, _vp, C.c_double, C.c_double, _vp, _vp, C.c_int, _vp]),
     "qx_set_shard": (C.c_int, [_vp, C.c_int, C.c_int]),
     "qx_partition_costs": (C.c_int, [_vp, C.c_longlong, C.c_int, _vp]),
     "qx_engine_config": (C.c_int, [_vp, C.c_int, _vp]),

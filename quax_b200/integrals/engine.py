@@ -167,6 +167,22 @@ class EriEngine:
             out["%d%d%d%d" % c["l"]] = (self.ENGINE_NAMES[cfg[0]], int(cfg[1]), self.ENGINE_NAMES[cfg[2]], int(cfg[3]))
         return out
 
+    def grad_adjoint_jvp(self, D: torch.Tensor, v, cj: float = 1.0, ck: float = -0.5, stream=None) -> torch.Tensor:
+        """Hessian-vector product of sum Gamma G (Gamma from D, fixed) along v (3N)."""
+        D = D.to(device=self.device, dtype=torch.float64).contiguous()
+        v = torch.as_tensor(v, dtype=torch.float64).to(self.device).contiguous().reshape(-1)
+        if v.numel() != 3 * self.natom:
+            raise ValueError(f"v has {v.numel()} entries, expected {3 * self.natom}")
+        out = torch.empty(3 * self.natom, dtype=torch.float64, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.check(
+                _lib.load().qx_grad_adjoint_jvp(self.handle, C.c_void_p(D.data_ptr()), float(cj), float(ck),
+                                                C.c_void_p(v.data_ptr()), C.c_void_p(out.data_ptr()), 1,
+                                                C.c_void_p(_stream_ptr(stream))),
+                "qx_grad_adjoint_jvp",
+            )
+        return out
+
     def grad_adjoint_class(self, cls: int, D: torch.Tensor, grad: torch.Tensor, cj: float = 1.0, ck: float = -0.5,
                            stream=None) -> torch.Tensor:
         """Adds one class's adjoint-gradient contribution into grad (3N, device)."""

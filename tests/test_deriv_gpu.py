@@ -159,3 +159,55 @@ def test_deriv_errors():
         eng.eri_deriv(dv)
     with pytest.raises(ValueError):
         eng.eri_deriv(np.zeros(5, dtype=int))
+
+
+def _unpack_hessian_slices(d2, M):
+    """(M(M+1)/2, ...) unique nu1 <= nu2 slices -> (M, M, ...) symmetric."""
+    H = np.zeros((M, M) + d2.shape[1:])
+    r = 0
+    for a in range(M):
+        for c in range(a, M):
+            H[a, c] = H[c, a] = d2[r]
+            r += 1
+    return H
+
+
+@pytest.mark.parametrize("seed", [0, 3])
+def test_grad_adjoint_jvp(seed):
+    """Hessian-vector product of sum Gamma G (Gamma fixed) against (a) the order-2
+    tensor contracted with Gamma and v, and (b) central differences of the adjoint
+    gradient along v (h = 1e-4 bohr; tolerance 1e-6 relative)."""
+    b = sp_synthetic(seed)
+    eng = _engine(b, 1e-12)
+    n, M = eng.nbf, 3 * b.natom
+    D = density(n, seed)
+    Dt = torch.from_numpy(D).cuda()
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=M)
+    hv = eng.grad_adjoint_jvp(Dt, v, 1.0, -0.5).cpu().numpy()
+    # (a) dense order-2 tensor
+    H = _unpack_hessian_slices(eng.eri_deriv_core(2).cpu().numpy(), M)
+    Gam = np.einsum("ij,kl->ijkl", D, D) - 0.5 * np.einsum("ik,jl->ijkl", D, D)
+    HG = np.einsum("abijkl,ijkl->ab", H, Gam)
+    assert np.abs(hv - HG @ v).max() < 1e-9 * max(1.0, np.abs(HG).max())
+    # (b) central differences of the adjoint gradient
+    h = 1e-4
+    X = b.atom_coords().reshape(-1)
+    gp = _engine(b.with_coords((X + h * v).reshape(-1, 3)), 1e-12).grad_adjoint(Dt, 1.0, -0.5).cpu().numpy()
+    gm = _engine(b.with_coords((X - h * v).reshape(-1, 3)), 1e-12).grad_adjoint(Dt, 1.0, -0.5).cpu().numpy()
+    fd = (gp - gm) / (2 * h)
+    assert np.abs(hv - fd).max() < 1e-6 * max(1.0, np.abs(fd).max())
+    # a unit vector gives one Hessian column
+    e0 = np.zeros(M)
+    e0[1] = 1.0
+    col = eng.grad_adjoint_jvp(Dt, e0, 1.0, -0.5).cpu().numpy()
+    assert np.abs(col - HG[:, 1]).max() < 1e-9 * max(1.0, np.abs(HG).max())
+
+
+def test_grad_adjoint_jvp_errors():
+    eng = _engine(small_synthetic(0), 1e-12)  # d shells: no order-2 programs in this build
+    D = torch.eye(eng.nbf, dtype=torch.float64).cuda()
+    with pytest.raises(NotImplementedError):
+        eng.grad_adjoint_jvp(D, np.zeros(3 * eng.natom))
+    with pytest.raises(ValueError):
+        eng.grad_adjoint_jvp(D, np.zeros(5))
