@@ -171,6 +171,18 @@ int qx_grad_adjoint_class(qx_handle *h, int cls, const double *D_dev, double cj,
 int qx_set_shard(qx_handle *h, int rank, int nranks);
 int qx_partition_costs(const double *cost, long long n, int nranks, long long *bounds);
 
+/* Mixed precision, no counterpart in the reference (Libint is FP64 throughout).
+ * Quartets whose Schwarz bound sqrt(K_ab K_cd) is below `bound` run their
+ * Obara-Saika recurrences in FP32 on the warp and split engines; the primitive
+ * set-up, the Boys function, the sums over primitives, the HRR, the epilogues and
+ * every accumulation into J, K, gradients and tensors stay FP64.  Each class's
+ * list is reordered with its FP64 quartets first, which reorders the unique
+ * layout.  bound <= 0 (the default) keeps everything FP64.  Synchronises the
+ * device; call qx_autotune afterwards.  qx_precision_split returns how many of a
+ * class's quartets (in this rank's view) stay FP64. */
+int qx_set_precision(qx_handle *h, double bound);
+long long qx_precision_split(const qx_handle *h, int cls);
+
 /* Autotuner, no counterpart in the reference.  Times, on this handle's own
  * quartet lists, every engine configuration each class can run and keeps the
  * fastest: straight-line kernels with 1..32 lanes per quartet, warp kernels with

@@ -72,15 +72,23 @@ XYZ = "xyz"
 
 
 class Emitter:
-    def __init__(self, prefix: str):
+    """SSA emitter.  ctype is the value type (the warp programs use the template
+    parameter T, so one program serves FP64 and FP32 recurrences); lit formats a
+    constant of that type."""
+
+    def __init__(self, prefix: str, ctype: str = "double"):
         self.lines: List[str] = []
         self.n = 0
         self.prefix = prefix
+        self.ctype = ctype
+
+    def lit(self, x: float) -> str:
+        return repr(float(x)) if self.ctype == "double" else f"{self.ctype}({float(x)!r})"
 
     def new(self, expr: str) -> str:
         name = f"{self.prefix}{self.n}"
         self.n += 1
-        self.lines.append(f"const double {name} = {expr};")
+        self.lines.append(f"const {self.ctype} {name} = {expr};")
         return name
 
 
@@ -105,7 +113,7 @@ class VRR:
             if n >= 2:
                 em2 = sh(e, i, -2)
                 terms.append(
-                    f"{float(n - 1)!r} * q.oo2z * ({self.get(em2, f, m)} - q.roz * {self.get(em2, f, m + 1)})"
+                    f"{self.em.lit(n - 1)} * q.oo2z * ({self.get(em2, f, m)} - q.roz * {self.get(em2, f, m + 1)})"
                 )
             name = self.em.new(" + ".join(terms))
         else:
@@ -116,10 +124,10 @@ class VRR:
             if nf >= 2:
                 fm2 = sh(f, j, -2)
                 terms.append(
-                    f"{float(nf - 1)!r} * q.oo2e * ({self.get(e, fm2, m)} - q.roe * {self.get(e, fm2, m + 1)})"
+                    f"{self.em.lit(nf - 1)} * q.oo2e * ({self.get(e, fm2, m)} - q.roe * {self.get(e, fm2, m + 1)})"
                 )
             if e[j] >= 1:
-                terms.append(f"{float(e[j])!r} * q.oo2ze * {self.get(sh(e, j, -1), fm1, m + 1)}")
+                terms.append(f"{self.em.lit(e[j])} * q.oo2ze * {self.get(sh(e, j, -1), fm1, m + 1)}")
             name = self.em.new(" + ".join(terms))
         self.memo[key] = name
         return name
@@ -727,9 +735,9 @@ def _peak_live(lines, consumed_at):
     uses = {}
     defs = []
     for i, ln in enumerate(lines):
-        m = _re.match(r"const double (v\d+) = (.*);", ln)
+        m = _re.match(r"const \w+ (v\d+(?:_\d+)?) = (.*);", ln)
         body = m.group(2) if m else ln
-        for d in _re.findall(r"\b(v\d+)\b", body):
+        for d in _re.findall(r"\b(v\d+(?:_\d+)?)\b", body):
             uses[d] = i
         defs.append(m.group(1) if m else None)
     alive, pk = set(), 0
@@ -812,7 +820,7 @@ def warp_program(la, lb, lc, ld, deriv):
     lines = []
     peak = 0
     for ci, (c0, c1) in enumerate(chunks):
-        em = Emitter(f"v{ci}_" if len(chunks) > 1 else "v")
+        em = Emitter(f"v{ci}_" if len(chunks) > 1 else "v", "T")
         vr = VRR(em)
         for (e, f), sets in tlist[c0:c1]:
             v = vr.get(e, f, 0)
@@ -821,7 +829,9 @@ def warp_program(la, lb, lc, ld, deriv):
                 items.append((sp, e, f))
                 leaf[(sp, e, f)] = k
                 w = wname[sp]
-                em.lines.append(f"stg[{k % 16}] = {v};" if w is None else f"stg[{k % 16}] = {w} * {v};")
+                # items are staged and summed in FP64 whatever the recurrence type
+                em.lines.append(f"stg[{k % 16}] = (double){v};" if w is None
+                                else f"stg[{k % 16}] = {w} * (double){v};")
                 if k % 16 == 15:
                     em.lines.append(f"sink(stg, {k - 15}, lane);")
         peak = max(peak, _peak_live(em.lines, None))
@@ -834,8 +844,8 @@ def warp_program(la, lb, lc, ld, deriv):
             # compiler cannot merge this chunk's intermediates with an earlier
             # chunk's, whose values are dead by now
             lines.append("{")
-            lines.append(f"  double Fc[{S + 1}];")
-            lines.append("  PrimQ qc;")
+            lines.append(f"  T Fc[{S + 1}];")
+            lines.append("  PrimQT<T> qc;")
             lines.append(f"  qx_load_inputs<{S + 1}>(save, lane, qc, Fc);")
             for ln in em.lines:
                 ln = ln.replace("Fp[", "Fc[")
@@ -1037,9 +1047,10 @@ def gen_warp_code(cid, la, lb, lc, ld, deriv, p, want_warp=True, want_wvrr=False
         L.append(f"  static __device__ __forceinline__ const unsigned short* outs() {{ return k_ho_{tag}; }}")
     if want_wvrr and deriv:
         L.append(f"  static __device__ __forceinline__ const unsigned short* vmap() {{ return k_vm_{tag}; }}")
-    L.append("  template <class Q, class Sink>")
-    L.append("  static __device__ __forceinline__ void vrr(const double* __restrict__ Fp, const Q& q, double wa, double wb,"
-             " double wc, const Sink& sink, unsigned lane, double* save) {")
+    L.append("  // T = double, or float for the mixed-precision quartets (staging stays FP64)")
+    L.append("  template <class T, class Sink>")
+    L.append("  static __device__ __forceinline__ void vrr(const T* __restrict__ Fp, const PrimQT<T>& q, double wa,"
+             " double wb, double wc, const Sink& sink, unsigned lane, T* save) {")
     L.append("    (void)wa; (void)wb; (void)wc; (void)save;")
     L.append("    double stg[16];")
     L += ["    " + ln for ln in p["lines"]]

@@ -42,11 +42,26 @@ struct __align__(16) PairInfo {
 };
 
 // Per-primitive-quartet scalars consumed by the generated VRR.
-struct PrimQ {
-    double PAx, PAy, PAz, WPx, WPy, WPz;
-    double QCx, QCy, QCz, WQx, WQy, WQz;
-    double oo2z, roz, oo2e, roe, oo2ze;
+template <class T>
+struct PrimQT {
+    T PAx, PAy, PAz, WPx, WPy, WPz;
+    T QCx, QCy, QCz, WQx, WQy, WQz;
+    T oo2z, roz, oo2e, roe, oo2ze;
 };
+using PrimQ = PrimQT<double>;
+
+// FP32 copy of the VRR scalars (mixed precision: the set-up and the Boys
+// function stay FP64, the recurrences run in FP32).
+__device__ __forceinline__ PrimQT<float> qx_to_float(const PrimQ& q) {
+    PrimQT<float> r;
+    r.PAx = (float)q.PAx; r.PAy = (float)q.PAy; r.PAz = (float)q.PAz;
+    r.WPx = (float)q.WPx; r.WPy = (float)q.WPy; r.WPz = (float)q.WPz;
+    r.QCx = (float)q.QCx; r.QCy = (float)q.QCy; r.QCz = (float)q.QCz;
+    r.WQx = (float)q.WQx; r.WQy = (float)q.WQy; r.WQz = (float)q.WQz;
+    r.oo2z = (float)q.oo2z; r.roz = (float)q.roz; r.oo2e = (float)q.oo2e;
+    r.roe = (float)q.roe; r.oo2ze = (float)q.oo2ze;
+    return r;
+}
 
 // Boys function F_0..F_S(T): 8-term Taylor expansion of the top order about the
 // nearest grid point (dF_m/dT = -F_{m+1}), then downward recursion

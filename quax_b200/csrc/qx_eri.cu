@@ -215,6 +215,9 @@ struct ClassWork {
     // buffers; task quartet indices are relative to their slice
     std::vector<long long> slice_q, slice_t;  // quartet / task boundaries, nslice + 1 each
     double* d_pacc = nullptr;  // plain split-mode accumulators (one slice)
+    // mixed precision: the full list holds its FP64 quartets first; n64_full of
+    // them, nq64 in this rank's view
+    long long n64_full = 0x7fffffffffffffffLL, nq64 = 0x7fffffffffffffffLL;
 };
 
 // Bytes of accumulator buffer the split modes may use per class.
@@ -261,6 +264,8 @@ struct qx_handle {
     int deriv_eng[QX_NUM_CLASSES];
     int wpq[QX_NUM_CLASSES];        // warps per quartet, plain warp kernels
     int wpq_deriv[QX_NUM_CLASSES];  // warps per quartet, derivative warp kernels
+    int shard_rank = 0, shard_n = 1;
+    double f32_bound = 0.0;  // mixed precision: FP32 recurrences below this Schwarz bound
 };
 
 // Primitive-chunk tasks (quartet, first primitive quartet) and the accumulator
@@ -391,6 +396,7 @@ static int run_class(qx_handle* h, int cls, int mode, const int2* d_q, long long
     a.dens = dens;
     a.log2g = eng == ENG_SL ? log2g : 0;
     a.err = h->d_err;
+    if (d_q == h->work[cls].d_q) a.nq64 = h->work[cls].nq64;
     if (eng == ENG_COOP) {
         qx_launch_coop(g_coop_idx[cls], a, mode, s);
     } else if (eng == ENG_WARP || eng == ENG_WSPLIT) {
@@ -696,20 +702,16 @@ extern "C" int qx_partition_costs(const double* cost, long long n, int nranks, l
     return QX_OK;
 }
 
-// Restrict the handle to rank `rank` of `nranks`: every class keeps a
-// cost-balanced contiguous range of its screened quartets (cost = primitive
-// quartets), so the ranks' results (dense tensors, derivative tensors, J, K,
-// gradients) sum to the full one.  The unique layout then holds this rank's
-// quartets only.  nranks = 1 restores the full lists.
-extern "C" int qx_set_shard(qx_handle* h, int rank, int nranks) {
-    if (!h || nranks < 1 || rank < 0 || rank >= nranks) return fail(QX_E_INVALID, "qx_set_shard: bad rank/nranks");
-    DeviceGuard g(h->device);
+// Recompute every class's view (this rank's contiguous range of the full list,
+// with its FP64/FP32 boundary) and the unique layout; split-mode buffers belong to
+// the old view and are dropped.
+static int rebuild_views(qx_handle* h) {
     QX_CUDA(cudaDeviceSynchronize());
+    const int rank = h->shard_rank, nranks = h->shard_n;
     long long base = 0;
     h->nunique = 0;
     for (int c = 0; c < QX_NUM_CLASSES; ++c) {
         ClassWork& w = h->work[c];
-        // split-mode buffers belong to the old range
         cudaFree(w.d_dtasks);
         cudaFree(w.d_dacc);
         cudaFree(w.d_pacc);
@@ -736,12 +738,64 @@ extern "C" int qx_set_shard(qx_handle* h, int rank, int nranks) {
         w.d_q = w.d_q_full + lo;
         w.nq = hi - lo;
         w.prims = prims;
+        w.nq64 = w.n64_full >= hi ? 0x7fffffffffffffffLL : std::max(0LL, w.n64_full - lo);
         w.unique_base = base;
         base += w.nq * g_class_nout[c];
         h->nunique += w.nq;
     }
     h->unique_size = base;
     return QX_OK;
+}
+
+// Restrict the handle to rank `rank` of `nranks`: every class keeps a
+// cost-balanced contiguous range of its screened quartets (cost = primitive
+// quartets), so the ranks' results (dense tensors, derivative tensors, J, K,
+// gradients) sum to the full one.  The unique layout then holds this rank's
+// quartets only.  nranks = 1 restores the full lists.
+extern "C" int qx_set_shard(qx_handle* h, int rank, int nranks) {
+    if (!h || nranks < 1 || rank < 0 || rank >= nranks) return fail(QX_E_INVALID, "qx_set_shard: bad rank/nranks");
+    DeviceGuard g(h->device);
+    h->shard_rank = rank;
+    h->shard_n = nranks;
+    return rebuild_views(h);
+}
+
+// Mixed precision: quartets whose Schwarz bound sqrt(K_ab K_cd) is below `bound`
+// run their recurrences in FP32 (warp and split engines; set-up, Boys function,
+// accumulation over primitives, HRR and epilogues stay FP64).  Each class's list
+// is reordered to hold its FP64 quartets first (both parts keep the
+// largest-primitive-count-first order), which also reorders the unique layout.
+// bound <= 0 makes every quartet FP64 again.
+extern "C" int qx_set_precision(qx_handle* h, double bound) {
+    if (!h || !std::isfinite(bound)) return fail(QX_E_INVALID, "qx_set_precision: bad argument");
+    DeviceGuard g(h->device);
+    QX_CUDA(cudaDeviceSynchronize());
+    h->f32_bound = bound > 0.0 ? bound : 0.0;
+    const double b2 = h->f32_bound * h->f32_bound;
+    const int ns = h->nshell;
+    auto kpair = [&](const PairInfo& p) { return h->K[(size_t)p.s1 * ns + p.s2]; };
+    for (int c = 0; c < QX_NUM_CLASSES; ++c) {
+        ClassWork& w = h->work[c];
+        if (!w.nq_full) continue;
+        std::vector<int2> L((size_t)w.nq_full);
+        QX_CUDA(cudaMemcpy(L.data(), w.d_q_full, sizeof(int2) * w.nq_full, cudaMemcpyDeviceToHost));
+        // restore the set-up order (bra nprim, then ket nprim, largest first), then
+        // split by the bound
+        auto key = [&](const int2& q) { return h->pairs[q.x].nprim * 64 + h->pairs[q.y].nprim; };
+        std::stable_sort(L.begin(), L.end(), [&](const int2& x, const int2& y) { return key(x) > key(y); });
+        auto is64 = [&](const int2& q) { return b2 <= 0.0 || kpair(h->pairs[q.x]) * kpair(h->pairs[q.y]) >= b2; };
+        auto mid = std::stable_partition(L.begin(), L.end(), is64);
+        const long long n64 = (long long)(mid - L.begin());
+        w.n64_full = n64 == w.nq_full ? 0x7fffffffffffffffLL : n64;
+        QX_CUDA(cudaMemcpy(w.d_q_full, L.data(), sizeof(int2) * w.nq_full, cudaMemcpyHostToDevice));
+    }
+    return rebuild_views(h);
+}
+
+extern "C" long long qx_precision_split(const qx_handle* h, int cls) {
+    if (!h || cls < 0 || cls >= QX_NUM_CLASSES) return fail(QX_E_INVALID, "qx_precision_split: bad argument");
+    const ClassWork& w = h->work[cls];
+    return w.nq64 >= w.nq ? w.nq : w.nq64;
 }
 
 extern "C" int qx_finalize(qx_handle* h) {
@@ -849,6 +903,7 @@ static EriArgs class_args(qx_handle* h, int c, double* out) {
     a.err = h->d_err;
     a.out2 = nullptr;
     a.dens = nullptr;
+    a.nq64 = w.nq64;
     return a;
 }
 
@@ -877,6 +932,7 @@ static int run_deriv_class(qx_handle* h, int c, int mode, double* out, const dou
             EriArgs a = class_args(h, c, out);
             a.quartets = w.d_q + w.slice_q[sl];
             a.nq = w.slice_q[sl + 1] - w.slice_q[sl];
+            a.nq64 = w.nq64 - w.slice_q[sl];
             const int2* tk = w.d_dtasks + w.slice_t[sl];
             const long long nt = w.slice_t[sl + 1] - w.slice_t[sl];
             if (h->deriv_eng[c] == ENG_WVRR) {

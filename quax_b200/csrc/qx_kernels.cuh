@@ -25,6 +25,9 @@ struct EriArgs {
     const double* dens; // MODE_JK: D
     int log2g;       // log2 of the lanes cooperating on one quartet (0..5)
     int* err;
+    // mixed precision: quartets [nq64, nq) of the list run their recurrences in
+    // FP32 (warp and split engines); the default keeps every quartet FP64
+    long long nq64 = 0x7fffffffffffffffLL;
 };
 
 // Accumulator storage for the contracted [e0|f0] targets of one quartet.

@@ -106,9 +106,9 @@ struct GlobalSink {
 // quartet (lane-strided, bank-conflict free) and every later chunk reloads them
 // with volatile loads, so the compiler cannot merge a chunk's recomputed
 // intermediates with an earlier chunk's and keep them all live.
-template <int NF>
-__device__ __forceinline__ void qx_save_inputs(const PrimQ& q, const double* Fp, double* save, unsigned lane) {
-    double* s = save + lane;
+template <int NF, class T>
+__device__ __forceinline__ void qx_save_inputs(const PrimQT<T>& q, const T* Fp, T* save, unsigned lane) {
+    T* s = save + lane;
     s[0 * 32] = q.PAx; s[1 * 32] = q.PAy; s[2 * 32] = q.PAz;
     s[3 * 32] = q.WPx; s[4 * 32] = q.WPy; s[5 * 32] = q.WPz;
     s[6 * 32] = q.QCx; s[7 * 32] = q.QCy; s[8 * 32] = q.QCz;
@@ -119,9 +119,9 @@ __device__ __forceinline__ void qx_save_inputs(const PrimQ& q, const double* Fp,
     for (int m = 0; m < NF; ++m) s[(17 + m) * 32] = Fp[m];
 }
 
-template <int NF>
-__device__ __forceinline__ void qx_load_inputs(const double* save, unsigned lane, PrimQ& q, double* F) {
-    const volatile double* s = save + lane;
+template <int NF, class T>
+__device__ __forceinline__ void qx_load_inputs(const T* save, unsigned lane, PrimQT<T>& q, T* F) {
+    const volatile T* s = save + lane;
     q.PAx = s[0 * 32]; q.PAy = s[1 * 32]; q.PAz = s[2 * 32];
     q.WPx = s[3 * 32]; q.WPy = s[4 * 32]; q.WPz = s[5 * 32];
     q.QCx = s[6 * 32]; q.QCy = s[7 * 32]; q.QCz = s[8 * 32];
@@ -203,6 +203,7 @@ __global__ void __launch_bounds__(WARP_QPB * 32) k_warp(WarpArgs wa, int mode) {
     const PairInfo P = a.pairs[pq.x];
     const PairInfo Q = a.pairs[pq.y];
     const int atA = P.atom1, atB = P.atom2, atC = Q.atom1, atD = Q.atom2;
+    const bool f32 = qi >= a.nq64;  // warp-uniform: one quartet per warp
     if (DERIV) {
         if (atA == atB && atA == atC && atA == atD) return;  // reference skips these
         if (mode == WMODE_DER_SLICE) {
@@ -238,7 +239,19 @@ __global__ void __launch_bounds__(WARP_QPB * 32) k_warp(WarpArgs wa, int mode) {
 #pragma unroll
             for (int m = 0; m <= W::S; ++m) Fp[m] = 0.0;
         }
-        W::vrr(Fp, q, 2.0 * p.alpha, 2.0 * (p.zeta - p.alpha), 2.0 * r.alpha, SmemSink{H}, lane, save);
+        const double w1 = 2.0 * p.alpha, w2 = 2.0 * (p.zeta - p.alpha), w3 = 2.0 * r.alpha;
+        if constexpr (DERIV < 2) {
+            if (f32) {
+                float Ff[W::S + 1];
+#pragma unroll
+                for (int m = 0; m <= W::S; ++m) Ff[m] = (float)Fp[m];
+                W::vrr(Ff, qx_to_float(q), w1, w2, w3, SmemSink{H}, lane, reinterpret_cast<float*>(save));
+            } else {
+                W::vrr(Fp, q, w1, w2, w3, SmemSink{H}, lane, save);
+            }
+        } else {
+            W::vrr(Fp, q, w1, w2, w3, SmemSink{H}, lane, save);
+        }
         __syncwarp();
     }
     if (wpq > 1) {
@@ -463,6 +476,7 @@ __global__ void __launch_bounds__(WARP_QPB * 32) k_gvrr(EriArgs a, const int2* _
     const PairInfo Q = a.pairs[pq.y];
     if (DER && P.atom1 == P.atom2 && P.atom1 == Q.atom1 && P.atom1 == Q.atom2) return;  // reference skips these
     double* qacc = acc + (size_t)task.x * (DER ? nacc : W::NITEM_PAD);
+    const bool f32 = task.x >= a.nq64;  // warp-uniform: one task per warp
     extern __shared__ double wv_sm[];
     double* save = wv_sm + (size_t)(threadIdx.x >> 5) * W::SAVE;
     const int nk = Q.nprim, ntot = P.nprim * nk;
@@ -482,10 +496,22 @@ __global__ void __launch_bounds__(WARP_QPB * 32) k_gvrr(EriArgs a, const int2* _
             for (int m = 0; m <= W::S; ++m) Fp[m] = 0.0;
         }
         const double wa = 2.0 * p.alpha, wb = 2.0 * (p.zeta - p.alpha), wc = 2.0 * r.alpha;
-        if constexpr (DER)
-            W::vrr(Fp, q, wa, wb, wc, GlobalSink{qacc, W::vmap()}, lane, save);
-        else
-            W::vrr(Fp, q, wa, wb, wc, IdentSink{qacc}, lane, save);
+        if (f32) {
+            float Ff[W::S + 1];
+#pragma unroll
+            for (int m = 0; m <= W::S; ++m) Ff[m] = (float)Fp[m];
+            const PrimQT<float> qf = qx_to_float(q);
+            float* sf = reinterpret_cast<float*>(save);
+            if constexpr (DER)
+                W::vrr(Ff, qf, wa, wb, wc, GlobalSink{qacc, W::vmap()}, lane, sf);
+            else
+                W::vrr(Ff, qf, wa, wb, wc, IdentSink{qacc}, lane, sf);
+        } else {
+            if constexpr (DER)
+                W::vrr(Fp, q, wa, wb, wc, GlobalSink{qacc, W::vmap()}, lane, save);
+            else
+                W::vrr(Fp, q, wa, wb, wc, IdentSink{qacc}, lane, save);
+        }
         __syncwarp();
     }
 }

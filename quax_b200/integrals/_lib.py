@@ -56,6 +56,8 @@ SIGNATURES = {
     "qx_autotune": (C.c_int, [_vp, C.c_int, _vp]),
     "qx_grad_adjoint_jvp": (C.c_int, [_vp, _vp, C.c_double, C.c_double, _vp, _vp, C.c_int, _vp]),
     "qx_set_shard": (C.c_int, [_vp, C.c_int, C.c_int]),
+    "qx_set_precision": (C.c_int, [_vp, C.c_double]),
+    "qx_precision_split": (C.c_longlong, [_vp, C.c_int]),
     "qx_partition_costs": (C.c_int, [_vp, C.c_longlong, C.c_int, _vp]),
     "qx_engine_config": (C.c_int, [_vp, C.c_int, _vp]),
     "qx_compute_2e_int_noalloc": (

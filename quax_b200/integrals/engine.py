@@ -76,6 +76,18 @@ class EriEngine:
         with torch.cuda.device(self.device):
             _lib.check(_lib.load().qx_set_shard(self.handle, int(rank), int(nranks)), "qx_set_shard")
 
+    def set_precision(self, f32_bound: float) -> None:
+        """Mixed precision: FP32 recurrences for quartets with Schwarz bound below
+        f32_bound (0 = all FP64).  Reorders the unique layout."""
+        with torch.cuda.device(self.device):
+            _lib.check(_lib.load().qx_set_precision(self.handle, float(f32_bound)), "qx_set_precision")
+
+    def precision_split(self):
+        """{"la lb lc ld": (FP64 quartets, all quartets)} of this handle's view."""
+        lib = _lib.load()
+        return {"%d%d%d%d" % c["l"]: (int(lib.qx_precision_split(self.handle, c["cls"])), c["nq"])
+                for c in self.class_info() if c["nq"]}
+
     def unique_quartets(self) -> int:
         return int(_lib.load().qx_unique_quartets(self.handle))
 
