@@ -173,7 +173,9 @@ int qx_partition_costs(const double *cost, long long n, int nranks, long long *b
 
 /* Mixed precision, no counterpart in the reference (Libint is FP64 throughout).
  * Quartets whose Schwarz bound sqrt(K_ab K_cd) is below `bound` run their
- * Obara-Saika recurrences in FP32 on the warp and split engines; the primitive
+ * Obara-Saika recurrences in FP32 on the warp and split engines, in classes
+ * whose HRR has at most two transfer steps (lb + ld <= 2: the HRR amplifies the
+ * FP32 error about tenfold per step, so the others stay FP64); the primitive
  * set-up, the Boys function, the sums over primitives, the HRR, the epilogues and
  * every accumulation into J, K, gradients and tensors stay FP64.  Each class's
  * list is reordered with its FP64 quartets first, which reorders the unique

@@ -783,7 +783,14 @@ extern "C" int qx_set_precision(qx_handle* h, double bound) {
         // split by the bound
         auto key = [&](const int2& q) { return h->pairs[q.x].nprim * 64 + h->pairs[q.y].nprim; };
         std::stable_sort(L.begin(), L.end(), [&](const int2& x, const int2& y) { return key(x) > key(y); });
-        auto is64 = [&](const int2& q) { return b2 <= 0.0 || kpair(h->pairs[q.x]) * kpair(h->pairs[q.y]) >= b2; };
+        // FP32 recurrence errors are amplified by the HRR's cancellations, about
+        // tenfold per transfer step (measured relative error of the FP32 path:
+        // <= 4e-5 with lb + ld <= 1, ~2e-3 with 2, 1e-1 with 3, above 1 with 4), so
+        // classes with more than two transfer steps stay FP64
+        const bool eligible = g_class_l[c][1] + g_class_l[c][3] <= 2;
+        auto is64 = [&](const int2& q) {
+            return !eligible || b2 <= 0.0 || kpair(h->pairs[q.x]) * kpair(h->pairs[q.y]) >= b2;
+        };
         auto mid = std::stable_partition(L.begin(), L.end(), is64);
         const long long n64 = (long long)(mid - L.begin());
         w.n64_full = n64 == w.nq_full ? 0x7fffffffffffffffLL : n64;

@@ -2,10 +2,10 @@
 threshold run their recurrences in FP32, everything else FP64.
 
 Every result is compared with the all-FP64 GPU run of the same handle, and the
-error is bounded in terms of the threshold: on these molecules the FP32
-recurrences lose up to ~2e-3 of the quartet's bound (cancellation between the
-recurrence terms), so the tests allow 5e-3 x bound per integral, and the J/K,
-energy and gradient errors that follow from it.  With the threshold at 0 the
+error is bounded in terms of the threshold: in the classes that may run FP32
+(HRR with at most two transfer steps) the FP32 recurrences lose up to ~2e-3 of
+the integral's magnitude, itself below the quartet's bound, so the tests allow
+5e-3 x bound per integral, and the J/K and gradient errors that follow from it.  With the threshold at 0 the
 results must be the FP64 ones."""
 import numpy as np
 import pytest
