@@ -264,20 +264,24 @@ def run_ours(args):
 
     e2e_step()
     barrier()
-    t0 = time.perf_counter()
-    e2e_steps = max(1, min(args.steps, 3))
+    e2e_steps = max(3, min(args.steps, 5))
+    ts = []
     for _ in range(e2e_steps):
+        t0 = time.perf_counter()
         e2e_step()
-    barrier()
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
+        barrier()
+        ts.append(time.perf_counter() - t0)
+    e2e_s = statistics.median(ts)
     e2e = {"value": world * nq / e2e_s, "unit": "quartets/s", "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(8 * n**4), "ms_per_step": e2e_s * 1e3,
+           "ms_per_step_all": [round(t * 1e3, 2) for t in ts], "statistic": "median over steps (host wall clock)",
            "path": "qx_initialize + qx_compute_2e_int(host pinned n^4) + qx_finalize"}
     del host
 
     grad = None
     if not args.no_grad:
         grad = gradient_extras(eng, b, n, args.warmup)
+        grad["workload_30_atoms"] = gradient_30_atoms()
 
     cpu = cpu_baseline_eri(b) if rank == 0 else None
     if rank == 0:
@@ -351,6 +355,60 @@ def gradient_extras(eng, b, n, warmup):
         torch.cuda.empty_cache()
     else:
         out["plain_s"] = f"skipped: needs {need / 1e9:.0f} GB"
+    return out
+
+
+def gradient_30_atoms():
+    """The 30-atom adjoint-gradient workload: adjoint s/eval, and the plain path
+    timed on one of its 3N derivative slices (the full (3N, n^4) tensor is
+    ~12 TB), so plain_s is an estimate: 3N x one slice's compute + contraction."""
+    import numpy as np
+    import torch
+
+    from quax_b200.basis import config_spec, synthetic_molecule
+    from quax_b200.integrals.engine import EriEngine
+
+    mol, b = synthetic_molecule(config_spec("grad30"), 0)
+    eng = EriEngine(b, THR)
+    n = eng.nbf
+    rng = np.random.default_rng(0)
+    C = rng.normal(0.0, 1.0 / np.sqrt(n), size=(n, n // 4))
+    D = torch.from_numpy(C @ C.T).cuda()
+    eng.grad_adjoint(D)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    g = eng.grad_adjoint(D)
+    e1.record()
+    torch.cuda.synchronize()
+    adj = e0.elapsed_time(e1) * 1e-3
+    out = {"natom": b.natom, "nbf": n, "unique_quartets": eng.unique_quartets(), "adjoint_s": adj,
+           "plain_s_estimate": None}
+    free, _ = torch.cuda.mem_get_info()
+    if 8 * n**4 * 1.15 < free:
+        # plain path, one nuclear index: the n^4 slice, then sum Gamma dG with
+        # Gamma = D_ij D_kl - 1/2 D_ik D_jl contracted row block by row block
+        nu = 0
+        dv = np.zeros(3 * b.natom, dtype=np.int64)
+        dv[nu] = 1
+        sl = torch.empty((n, n, n, n), dtype=torch.float64, device="cuda")
+        e0.record()
+        eng.eri_deriv(dv, out=sl)
+        acc = torch.zeros((), dtype=torch.float64, device="cuda")
+        for i0 in range(0, n, 16):
+            blk = sl[i0:i0 + 16]  # (bi, n, n, n)
+            acc += torch.einsum("ajkl,aj,kl->", blk, D[i0:i0 + 16], D)
+            acc -= 0.5 * torch.einsum("ajkl,ak,jl->", blk, D[i0:i0 + 16], D)
+        e1.record()
+        torch.cuda.synchronize()
+        one = e0.elapsed_time(e1) * 1e-3
+        out["plain_s_estimate"] = one * 3 * b.natom
+        out["plain_slice_s"] = one
+        out["slice_check_abs_diff"] = abs(float(acc) - float(g[nu]))
+        out["adjoint_speedup_vs_plain_estimate"] = out["plain_s_estimate"] / adj
+        del sl
+        torch.cuda.empty_cache()
+    eng.close()
     return out
 
 
