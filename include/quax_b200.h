@@ -150,6 +150,17 @@ int qx_class_info(const qx_handle *h, int cls, int *l4, long long *nquartets, lo
 int qx_grad_adjoint_jvp(qx_handle *h, const double *D, double cj, double ck, const double *v, double *Hv,
                         int on_device, void *stream);
 
+/* One-electron integrals (the reference's compute_1e_int("overlap"|"kinetic"|
+ * "potential"), libint_interface.cc:232-483, and oei_deriv_core(1), :2403-2579),
+ * on the device, Cartesian, same conventions as the two-electron integrals.
+ * qx_set_charges gives the nuclear charges (natom doubles; the reference reads
+ * them from the xyz file) and must precede them.  qx_oei writes any of S, T, V
+ * (n x n, device, NULL to skip); qx_oei_deriv_core writes the three (3N, n, n)
+ * first-derivative tensors, nuclear index 3*atom + xyz. */
+int qx_set_charges(qx_handle *h, const double *Z);
+int qx_oei(qx_handle *h, double *S, double *T, double *V, void *stream);
+int qx_oei_deriv_core(qx_handle *h, int order, double *dS, double *dT, double *dV, void *stream);
+
 /* qx_eri_unique restricted to one class (same output positions). */
 int qx_eri_unique_class(qx_handle *h, int cls, double *out_dev, void *stream);
 

@@ -265,6 +265,9 @@ struct qx_handle {
     int wpq[QX_NUM_CLASSES];        // warps per quartet, plain warp kernels
     int wpq_deriv[QX_NUM_CLASSES];  // warps per quartet, derivative warp kernels
     int shard_rank = 0, shard_n = 1;
+    // one-electron integrals: nuclear charges and positions on the device
+    double* d_Z = nullptr;
+    double* d_xyz = nullptr;
     double f32_bound = 0.0;  // mixed precision: FP32 recurrences below this Schwarz bound
 };
 
@@ -369,6 +372,8 @@ static void free_handle(qx_handle* h) {
         if (h->done[i]) cudaEventDestroy(h->done[i]);
     }
     if (h->start) cudaEventDestroy(h->start);
+    cudaFree(h->d_Z);
+    cudaFree(h->d_xyz);
     delete h;
 }
 
@@ -1144,6 +1149,54 @@ extern "C" int qx_grad_adjoint_jvp(qx_handle* h, const double* D, double cj, dou
     cudaFree(dh);
     if (!rc) rc = check_err_word(h, s);
     return rc;
+}
+
+// ------------------------------------------------------ one-electron integrals --
+void qx_launch_oei(const qx::PairInfo* pairs, int npair, const qx::PrimPair* prims, const double* boys,
+                   const double* xyz, const double* Z, int natom, long long n, double* S, double* T, double* V,
+                   double* dS, double* dT, double* dV, cudaStream_t s);
+
+extern "C" int qx_set_charges(qx_handle* h, const double* Z) {
+    if (!h || !Z) return fail(QX_E_INVALID, "qx_set_charges: NULL argument");
+    for (int i = 0; i < h->natom; ++i)
+        if (!std::isfinite(Z[i])) return fail(QX_E_INVALID, "qx_set_charges: non-finite charge %d", i);
+    DeviceGuard g(h->device);
+    if (!h->d_Z && (cudaMalloc((void**)&h->d_Z, sizeof(double) * h->natom) != cudaSuccess ||
+                    cudaMalloc((void**)&h->d_xyz, sizeof(double) * 3 * h->natom) != cudaSuccess)) {
+        cudaGetLastError();
+        cudaFree(h->d_Z);
+        h->d_Z = nullptr;
+        return fail(QX_E_NOMEM, "qx_set_charges: allocation failed");
+    }
+    QX_CUDA(cudaMemcpy(h->d_Z, Z, sizeof(double) * h->natom, cudaMemcpyHostToDevice));
+    QX_CUDA(cudaMemcpy(h->d_xyz, h->coords.data(), sizeof(double) * 3 * h->natom, cudaMemcpyHostToDevice));
+    return QX_OK;
+}
+
+extern "C" int qx_oei(qx_handle* h, double* S, double* T, double* V, void* stream) {
+    if (!h) return fail(QX_E_INVALID, "qx_oei: NULL handle");
+    if (!h->d_Z) return fail(QX_E_INVALID, "qx_oei: nuclear charges not set (qx_set_charges)");
+    DeviceGuard g(h->device);
+    qx_launch_oei(h->d_pairs, (int)h->pairs.size(), h->d_prims, h->d_boys, h->d_xyz, h->d_Z, h->natom, h->nbf, S, T,
+                  V, nullptr, nullptr, nullptr, (cudaStream_t)stream);
+    QX_CUDA(cudaGetLastError());
+    return QX_OK;
+}
+
+extern "C" int qx_oei_deriv_core(qx_handle* h, int order, double* dS, double* dT, double* dV, void* stream) {
+    if (!h || !dS || !dT || !dV) return fail(QX_E_INVALID, "qx_oei_deriv_core: NULL argument");
+    if (order != 1) return fail(QX_E_UNSUPPORTED, "qx_oei_deriv_core: derivative order %d (this build: 1)", order);
+    if (!h->d_Z) return fail(QX_E_INVALID, "qx_oei_deriv_core: nuclear charges not set (qx_set_charges)");
+    DeviceGuard g(h->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t bytes = sizeof(double) * 3 * h->natom * (size_t)h->nbf * h->nbf;
+    QX_CUDA(cudaMemsetAsync(dS, 0, bytes, s));
+    QX_CUDA(cudaMemsetAsync(dT, 0, bytes, s));
+    QX_CUDA(cudaMemsetAsync(dV, 0, bytes, s));
+    qx_launch_oei(h->d_pairs, (int)h->pairs.size(), h->d_prims, h->d_boys, h->d_xyz, h->d_Z, h->natom, h->nbf,
+                  nullptr, nullptr, nullptr, dS, dT, dV, s);
+    QX_CUDA(cudaGetLastError());
+    return QX_OK;
 }
 
 // ---------------------------------------------------------------- class info ---

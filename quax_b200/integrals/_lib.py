@@ -54,6 +54,9 @@ SIGNATURES = {
     "qx_eri_unique_class": (C.c_int, [_vp, C.c_int, _vp, _vp]),
     "qx_grad_adjoint_class": (C.c_int, [_vp, C.c_int, _vp, C.c_double, C.c_double, _vp, _vp]),
     "qx_autotune": (C.c_int, [_vp, C.c_int, _vp]),
+    "qx_set_charges": (C.c_int, [_vp, _vp]),
+    "qx_oei": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "qx_oei_deriv_core": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, _vp]),
     "qx_grad_adjoint_jvp": (C.c_int, [_vp, _vp, C.c_double, C.c_double, _vp, _vp, C.c_int, _vp]),
     "qx_set_shard": (C.c_int, [_vp, C.c_int, C.c_int]),
     "qx_set_precision": (C.c_int, [_vp, C.c_double]),

@@ -70,6 +70,35 @@ class EriEngine:
         return self._h
 
     # -- queries --------------------------------------------------------------
+    # -- one-electron integrals ---------------------------------------------
+    def set_charges(self, Z) -> None:
+        """Nuclear charges (natom) for the nuclear-attraction integrals."""
+        z = np.ascontiguousarray(np.asarray(Z, dtype=np.float64).reshape(-1))
+        if z.size != self.natom:
+            raise ValueError(f"{z.size} charges for {self.natom} atoms")
+        with torch.cuda.device(self.device):
+            _lib.check(_lib.load().qx_set_charges(self.handle, C.c_void_p(z.ctypes.data)), "qx_set_charges")
+
+    def oei(self, stream=None):
+        """(S, T, V), each (n, n) on the device."""
+        n = self.nbf
+        S, T, V = (torch.empty((n, n), dtype=torch.float64, device=self.device) for _ in range(3))
+        with torch.cuda.device(self.device):
+            _lib.check(_lib.load().qx_oei(self.handle, C.c_void_p(S.data_ptr()), C.c_void_p(T.data_ptr()),
+                                          C.c_void_p(V.data_ptr()), C.c_void_p(_stream_ptr(stream))), "qx_oei")
+        return S, T, V
+
+    def oei_deriv(self, order: int = 1, stream=None):
+        """(dS, dT, dV), each (3N, n, n) on the device."""
+        n = self.nbf
+        shape = (3 * self.natom, n, n)
+        dS, dT, dV = (torch.empty(shape, dtype=torch.float64, device=self.device) for _ in range(3))
+        with torch.cuda.device(self.device):
+            _lib.check(_lib.load().qx_oei_deriv_core(self.handle, int(order), C.c_void_p(dS.data_ptr()),
+                                                     C.c_void_p(dT.data_ptr()), C.c_void_p(dV.data_ptr()),
+                                                     C.c_void_p(_stream_ptr(stream))), "qx_oei_deriv_core")
+        return dS, dT, dV
+
     def set_shard(self, rank: int, nranks: int) -> None:
         """Keep a cost-balanced contiguous range of every class's quartets (rank of
         nranks); results of the ranks then sum to the full ones."""

@@ -8,6 +8,9 @@ quax/integrals/libint_interface.cc:2784-2807, backed by libquax_b200.so:
     compute_2e_int("eri", beta)          -> 1-D float64 array of n^4     (:486-647)
     compute_2e_deriv("eri", beta, deriv_vec) -> 1-D array of n^4        (:1097-1335)
     eri_deriv_core(deriv_order)          -> 1-D array of nderiv*n^4      (:2582-2779)
+    compute_1e_int(type)                 -> 1-D array of n^2 (overlap | kinetic | potential)  (:232-483)
+    compute_1e_deriv(type, deriv_vec)    -> 1-D array of n^2 (first order)                   (:650-788)
+    oei_deriv_core(deriv_order)          -> [overlap, kinetic, potential] nderiv*n^2 each    (:2403-2579)
     generate_multi_index_lookup(nparams, order) -> list of lists        (utils.h:158-172)
     LIBINT2_MAX_DERIV_ORDER                                              (:2806)
 
@@ -39,14 +42,17 @@ def initialize(xyzfilename: str, basis1: str, basis2: str, basis3: str, basis4: 
     if not (basis1 == basis2 == basis3 == basis4):
         raise NotImplementedError("the ERI path uses one basis for all four centres (quax/methods/ints.py:20)")
     mol = Molecule.from_xyz(xyzfilename, units="angstrom")
-    initialize_basis(build_basis(mol, basis1), ints_tol)
+    initialize_basis(build_basis(mol, basis1), ints_tol, charges=mol.Z)
 
 
-def initialize_basis(basis: Basis, ints_tol: float) -> None:
-    """Same as initialize() for an in-memory basis (coordinates in bohr)."""
+def initialize_basis(basis: Basis, ints_tol: float, charges=None) -> None:
+    """Same as initialize() for an in-memory basis (coordinates in bohr); the nuclear
+    charges are needed only for the potential integrals."""
     finalize()
     _state["engine"] = EriEngine(basis, ints_tol)
     _state["natom"] = basis.natom
+    if charges is not None:
+        _state["engine"].set_charges(charges)
 
 
 def finalize() -> None:
@@ -92,6 +98,39 @@ def eri_deriv_core(deriv_order: int) -> np.ndarray:
     out = eng.eri_deriv_core(deriv_order)
     assert out.shape[0] == how_many_derivs(eng.natom, deriv_order)
     return out.reshape(-1).cpu().numpy()
+
+
+_OEI_TYPES = ("overlap", "kinetic", "potential")
+
+
+def _oei_index(type_: str) -> int:
+    if type_ not in _OEI_TYPES:
+        raise ValueError("type must be overlap, kinetic, or potential")
+    return _OEI_TYPES.index(type_)
+
+
+def compute_1e_int(type_: str) -> np.ndarray:
+    return _engine().oei()[_oei_index(type_)].reshape(-1).cpu().numpy()
+
+
+def compute_1e_deriv(type_: str, deriv_vec) -> np.ndarray:
+    k = _oei_index(type_)
+    eng = _engine()
+    dv = np.asarray(deriv_vec, dtype=int).reshape(-1)
+    if dv.size != 3 * eng.natom:
+        raise ValueError("Derivative vector incorrect size for this molecule.")
+    order = int(dv.sum())
+    if order == 0:
+        return compute_1e_int(type_)
+    if order != 1 or (dv < 0).any():
+        raise NotImplementedError(f"one-electron derivative order {order} (this build: 1)")
+    return eng.oei_deriv(1)[k][int(np.argmax(dv))].reshape(-1).cpu().numpy()
+
+
+def oei_deriv_core(deriv_order: int):
+    if deriv_order != 1:
+        raise NotImplementedError(f"one-electron derivative order {deriv_order} (this build: 1)")
+    return [x.reshape(-1).cpu().numpy() for x in _engine().oei_deriv(1)]
 
 
 def generate_multi_index_lookup(nparams: int, deriv_order: int):

@@ -12,7 +12,7 @@ the SCF uses DIIS extrapolation, and the geometric gradient is analytic,
 with the two-electron term from the adjoint kernel (qx_grad_adjoint), so the
 3N x n^4 derivative tensor is never formed (the reference forms it and
 differentiates through every SCF iteration with jacfwd).  One-electron integrals
-are host-side (quax_b200.oei).
+and their derivatives come from the GPU kernel (qx_oei, qx_oei_deriv_core).
 """
 from __future__ import annotations
 
@@ -23,7 +23,7 @@ import torch
 
 from ..basis import Basis, Molecule
 from ..integrals.engine import EriEngine
-from ..oei import nuclear_repulsion, one_electron
+from ..oei import nuclear_repulsion
 
 
 @dataclass
@@ -38,10 +38,11 @@ class RHFResult:
 
 def restricted_hartree_fock(mol: Molecule, basis: Basis, ints_tol: float = 1.0e-14, maxit: int = 100,
                             conv: float = 1.0e-10, engine: EriEngine | None = None, device: str = "cuda") -> RHFResult:
-    S, T, V = one_electron(basis, mol.Z, mol.coords)
     dev = torch.device(device)
-    St, H = (torch.from_numpy(x).to(dev) for x in (S, T + V))
     eng = engine if engine is not None else EriEngine(basis, ints_tol, device=dev)
+    eng.set_charges(mol.Z)
+    St, T, V = eng.oei()
+    H = T + V
     A = torch.linalg.inv(torch.linalg.cholesky(St)).T
     ndocc = mol.nelectron // 2
     Enuc = nuclear_repulsion(mol.Z, mol.coords)
@@ -95,9 +96,9 @@ def rhf_gradient(mol: Molecule, basis: Basis, ints_tol: float = 1.0e-14, conv: f
     Cocc = res.C[:, :ndocc]
     D = Cocc @ Cocc.T
     W = Cocc @ torch.diag(res.eps[:ndocc]) @ Cocc.T
-    _, _, _, dS, dT, dV = one_electron(basis, mol.Z, mol.coords, deriv=True)
-    Dh, Wh = D.cpu().numpy(), W.cpu().numpy()
-    g = 2.0 * np.einsum("xij,ij->x", dT + dV, Dh) - 2.0 * np.einsum("xij,ij->x", dS, Wh)
-    g += res.engine.grad_adjoint(D, 2.0, -1.0).cpu().numpy()
+    res.engine.set_charges(mol.Z)
+    dS, dT, dV = res.engine.oei_deriv(1)
+    g = 2.0 * torch.einsum("xij,ij->x", dT + dV, D) - 2.0 * torch.einsum("xij,ij->x", dS, W)
+    g = (g + res.engine.grad_adjoint(D, 2.0, -1.0)).cpu().numpy()
     g += nuclear_repulsion(mol.Z, mol.coords, deriv=True)[1]
     return res.energy, g
