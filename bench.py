@@ -282,6 +282,7 @@ def run_ours(args):
     if not args.no_grad:
         grad = gradient_extras(eng, b, n, args.warmup)
         grad["workload_30_atoms"] = gradient_30_atoms()
+        grad["batched_rhf"] = batched_extras(args.batch)
 
     cpu = cpu_baseline_eri(b) if rank == 0 else None
     if rank == 0:
@@ -412,6 +413,46 @@ def gradient_30_atoms():
     return out
 
 
+def batched_extras(count: int, iterations: int = 20):
+    """Batched RHF: `count` Gaussian-displaced geometries (sigma 0.05 bohr) of one
+    12-atom synthetic molecule, J/K of the whole batch replayed from one CUDA graph
+    per SCF iteration, then the analytic gradients."""
+    import torch
+
+    from quax_b200.basis import SyntheticSpec, synthetic_molecule
+    from quax_b200.methods.batch import BatchedRHF, displaced_geometries
+
+    spec = SyntheticSpec(natom=12)
+    mol0, b0 = synthetic_molecule(spec, 0)
+    mols = displaced_geometries(mol0, count, 0.05, seed=1)
+    bases = [b0.with_coords(m.coords) for m in mols]
+    t0 = time.perf_counter()
+    br = BatchedRHF(mols, bases, ints_tol=THR)
+    nq = sum(m.eng.unique_quartets() for m in br.mols)
+    # eager J/K of the batch, for comparison with the graph replay
+    br._jk_all()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    br._jk_all()
+    e1.record()
+    torch.cuda.synchronize()
+    eager_ms = e0.elapsed_time(e1)
+    t1 = time.perf_counter()
+    E, t_jk = br.scf(iterations=iterations, use_graph=True)
+    t2 = time.perf_counter()
+    G = br.gradients()
+    torch.cuda.synchronize()
+    t3 = time.perf_counter()
+    br.close()
+    return {"molecules": count, "natom": mol0.natom, "nbf": b0.nbf(), "unique_quartets_per_jk": nq,
+            "scf_iterations": iterations, "setup_s": t1 - t0, "scf_s": t2 - t1,
+            "jk_graph_ms_per_iteration": t_jk / iterations * 1e3, "jk_eager_ms": eager_ms,
+            "jk_quartets_per_s": nq / (t_jk / iterations), "gradients_s": t3 - t2,
+            "energy_spread_Eh": float(max(E) - min(E)),
+            "max_abs_gradient": float(max(abs(g).max() for g in G))}
+
+
 def run_grad_only(args):
     """Adjoint gradient of the workload only (profiling aid; prints its timing)."""
     import numpy as np
@@ -485,6 +526,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-grad", action="store_true", help="skip the adjoint/plain gradient extras")
+    ap.add_argument("--batch", type=int, default=32,
+                    help="displaced geometries in the batched-RHF extra (the full workload is 256)")
     ap.add_argument("--profile-grad", action="store_true",
                     help="run only the adjoint gradient of the workload, warmup+steps times (for profiler runs)")
     ap.add_argument("--no-extras", action="store_true",
