@@ -278,6 +278,26 @@ def run_ours(args):
            "path": "qx_initialize + qx_compute_2e_int(host pinned n^4) + qx_finalize"}
     del host
 
+    # the same molecule with spherical d shells (the synthetic workload's basis):
+    # Cartesian kernels + per-class solid-harmonic transforms (batched GEMMs)
+    from quax_b200.basis import Basis
+    from quax_b200.integrals.spherical import SphericalEngine
+
+    sph = SphericalEngine(Basis(b.shells, b.natom, True, b.name), THR)
+    sph.cart.autotune(plain=True, deriv=False)
+    sph.eri_unique()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(3):
+        sph.eri_unique()
+    e1.record()
+    torch.cuda.synchronize()
+    sph_ms = e0.elapsed_time(e1) / 3
+    spherical = {"nbf": sph.nbf, "ms_per_step": sph_ms, "value": nq / (sph_ms * 1e-3), "unit": "quartets/s",
+                 "path": "Cartesian unique kernels + per-class solid-harmonic transforms (cuBLAS DGEMM)"}
+    sph.close()
+
     grad = None
     if not args.no_grad:
         grad = gradient_extras(eng, b, n, args.warmup)
@@ -308,6 +328,7 @@ def run_ours(args):
             "gpu_launches": launches,
             "clocks": clocks,
             "gradient": grad,
+            "spherical": spherical,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

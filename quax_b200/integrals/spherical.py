@@ -1,0 +1,160 @@
+"""Spherical (pure) basis functions on top of the Cartesian integral engine.
+
+The reference's Libint path is Cartesian (quax/integrals/libint_interface.cc:47-73
+calls set_pure(false)); the synthetic workloads with spherical d shells need the
+real-solid-harmonic functions.  Every quantity is the Cartesian one transformed
+with the block-diagonal matrix T (n_sph x n_cart) of the shells' solid
+harmonics:
+
+    G_sph = (T x T x T x T) G_cart          four quarter transforms (batched GEMMs)
+    J, K  = T J_cart(T^T D T) T^T,  ...      (J and K are linear in D)
+    grad  = grad_cart(T^T D T)              (Gamma built from D factorises)
+    S, T, V = T M T^T
+
+so the kernels stay Cartesian and the transforms are dense FP64 matrix products
+(cuBLAS DGEMM; FP64 tensor cores on B200).
+
+Conventions: Cartesian components in Libint's order, normalised so that x^l has
+unit norm; spherical functions in Libint's standard order m = -l..l, each of unit
+norm (for l = 1: y, z, x).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+from ..basis import Basis, cart_components
+from .engine import EriEngine
+
+
+def cart2sph(l: int) -> np.ndarray:
+    """(2l+1, ncart(l)) coefficients of the real solid harmonics over the Libint-
+    normalised Cartesian components."""
+    comps = cart_components(l)
+    idx = {c: k for k, c in enumerate(comps)}
+    M = np.zeros((2 * l + 1, len(comps)))
+    if l == 0:
+        M[0, 0] = 1.0
+    elif l == 1:
+        for m, c in enumerate(((0, 1, 0), (0, 0, 1), (1, 0, 0))):  # y, z, x
+            M[m, idx[c]] = 1.0
+    elif l == 2:
+        r3 = math.sqrt(3.0)
+        M[0, idx[(1, 1, 0)]] = r3                       # xy
+        M[1, idx[(0, 1, 1)]] = r3                       # yz
+        M[2, idx[(0, 0, 2)]] = 1.0                      # zz - (xx + yy) / 2
+        M[2, idx[(2, 0, 0)]] = -0.5
+        M[2, idx[(0, 2, 0)]] = -0.5
+        M[3, idx[(1, 0, 1)]] = r3                       # xz
+        M[4, idx[(2, 0, 0)]] = 0.5 * r3                 # (xx - yy) sqrt(3) / 2
+        M[4, idx[(0, 2, 0)]] = -0.5 * r3
+    else:
+        raise NotImplementedError("spherical functions for l <= 2")
+    return M
+
+
+def transform_matrix(basis: Basis) -> np.ndarray:
+    """Block-diagonal T (n_sph, n_cart) of a basis."""
+    blocks = [cart2sph(s.l) for s in basis.shells]
+    ns = sum(b.shape[0] for b in blocks)
+    nc = sum(b.shape[1] for b in blocks)
+    T = np.zeros((ns, nc))
+    r = c = 0
+    for b in blocks:
+        T[r:r + b.shape[0], c:c + b.shape[1]] = b
+        r += b.shape[0]
+        c += b.shape[1]
+    return T
+
+
+def _quarter(G: torch.Tensor, T: torch.Tensor, axis: int) -> torch.Tensor:
+    """Contract index `axis` of G with T (n_sph, n_cart): one batched GEMM."""
+    Gm = torch.movedim(G, axis, -1)
+    out = Gm @ T.T
+    return torch.movedim(out, -1, axis).contiguous()
+
+
+class SphericalEngine:
+    """Spherical-basis front of EriEngine: the Cartesian twin of the basis runs the
+    kernels, results are transformed with T."""
+
+    def __init__(self, basis: Basis, ints_tol: float = 1.0e-14, device=None):
+        if not basis.pure:
+            raise ValueError("SphericalEngine needs a pure basis")
+        cart = Basis(basis.shells, basis.natom, False, basis.name)
+        self.cart = EriEngine(cart, ints_tol, device)
+        self.device = self.cart.device
+        self.T = torch.from_numpy(transform_matrix(basis)).to(self.device)
+        self.nbf = self.T.shape[0]
+        self.natom = self.cart.natom
+        self.basis = basis
+
+    def close(self):
+        self.cart.close()
+
+    def set_charges(self, Z):
+        self.cart.set_charges(Z)
+
+    def autotune(self, **kw):
+        self.cart.autotune(**kw)
+
+    def _cart_density(self, D):
+        D = D.to(device=self.device, dtype=torch.float64)
+        return (self.T.T @ D @ self.T).contiguous()
+
+    # -- two-electron -------------------------------------------------------------
+    def eri(self) -> torch.Tensor:
+        G = self.cart.eri()
+        for ax in range(4):
+            G = _quarter(G, self.T, ax)
+        return G
+
+    def eri_unique(self):
+        """Per class, the spherical blocks of the screened unique quartets:
+        {(la,lb,lc,ld): (s_a, s_b, s_c, s_d, nq) tensor} -- the Cartesian unique
+        layout transformed class by class with batched GEMMs."""
+        out_c = torch.empty(self.cart.unique_size(), dtype=torch.float64, device=self.device)
+        self.cart.eri_unique(out_c)
+        res, base = {}, 0
+        for c in self.cart.class_info():
+            la, lb, lc, ld = c["l"]
+            dims = [(l + 1) * (l + 2) // 2 for l in (la, lb, lc, ld)]
+            size = int(np.prod(dims)) * c["nq"]
+            if c["nq"]:
+                blk = out_c[base:base + size].view(*dims, c["nq"])
+                for ax, l in enumerate((la, lb, lc, ld)):
+                    M = torch.from_numpy(cart2sph(l)).to(self.device)
+                    blk = _quarter(blk, M, ax)
+                res[(la, lb, lc, ld)] = blk
+            base += size
+        return res
+
+    def jk(self, D):
+        Jc, Kc = self.cart.jk(self._cart_density(D))
+        return self.T @ Jc @ self.T.T, self.T @ Kc @ self.T.T
+
+    def grad_adjoint(self, D, cj: float = 1.0, ck: float = -0.5):
+        return self.cart.grad_adjoint(self._cart_density(D), cj, ck)
+
+    def grad_adjoint_jvp(self, D, v, cj: float = 1.0, ck: float = -0.5):
+        return self.cart.grad_adjoint_jvp(self._cart_density(D), v, cj, ck)
+
+    def eri_deriv(self, deriv_vec) -> torch.Tensor:
+        G = self.cart.eri_deriv(deriv_vec)
+        for ax in range(4):
+            G = _quarter(G, self.T, ax)
+        return G
+
+    # -- one-electron -------------------------------------------------------------
+    def oei(self):
+        return tuple(self.T @ M @ self.T.T for M in self.cart.oei())
+
+    def oei_deriv(self, order: int = 1):
+        return tuple(torch.einsum("ai,xij,bj->xab", self.T, M, self.T) for M in self.cart.oei_deriv(order))
+
+
+def make_engine(basis: Basis, ints_tol: float = 1.0e-14, device=None):
+    """EriEngine for a Cartesian basis, SphericalEngine for a pure one."""
+    return SphericalEngine(basis, ints_tol, device) if basis.pure else EriEngine(basis, ints_tol, device)
