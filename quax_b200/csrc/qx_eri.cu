@@ -271,42 +271,58 @@ struct qx_handle {
     double f32_bound = 0.0;  // mixed precision: FP32 recurrences below this Schwarz bound
 };
 
-// Primitive-chunk tasks (quartet, first primitive quartet) and the accumulator
-// buffer of the split modes, built at the first call that needs them.  The
-// quartets are cut into slices of at most QX_SPLIT_ACC_BYTES of derivative
-// accumulators; each slice runs as its own VRR + HRR pair.
-static int ensure_split_tasks(qx_handle* h, int c) {
+// Primitive-chunk tasks (quartet, first primitive quartet) of the split modes,
+// built at set-up for the classes that use them by default and otherwise at the
+// first call that needs them; the derivative accumulator buffer is allocated at
+// the first derivative call (need_dacc).  The quartets are cut into slices of at
+// most QX_SPLIT_ACC_BYTES of derivative accumulators; each slice runs as its own
+// VRR + HRR pair.  `list` is the class's current view when the caller has it on
+// the host (set-up), else it is copied back from the device.
+static int ensure_split_tasks(qx_handle* h, int c, bool need_dacc = false, const int2* list = nullptr) {
     ClassWork& w = h->work[c];
-    if (w.d_dtasks || !w.nq) return QX_OK;
-    std::vector<int2> L((size_t)w.nq);
-    QX_CUDA(cudaMemcpy(L.data(), w.d_q, sizeof(int2) * w.nq, cudaMemcpyDeviceToHost));
+    if (!w.nq) return QX_OK;
     const long long nacc = qx_der_nacc(g_der_idx[c]);
     const long long cap_q = std::max(1LL, QX_SPLIT_ACC_BYTES / (8 * nacc));
-    std::vector<int2> tasks;
-    w.slice_q.assign(1, 0);
-    w.slice_t.assign(1, 0);
-    const int ch = qx_der_chunk();
-    long long q0 = 0;
-    for (long long qi = 0; qi < w.nq; ++qi) {
-        if (qi - q0 == cap_q) {
-            q0 = qi;
-            w.slice_q.push_back(qi);
-            w.slice_t.push_back((long long)tasks.size());
+    if (!w.d_dtasks) {
+        std::vector<int2> L;
+        if (!list) {
+            L.resize((size_t)w.nq);
+            QX_CUDA(cudaMemcpy(L.data(), w.d_q, sizeof(int2) * w.nq, cudaMemcpyDeviceToHost));
+            list = L.data();
         }
-        const int np_q = h->pairs[L[qi].x].nprim * h->pairs[L[qi].y].nprim;
-        for (int t0 = 0; t0 < np_q; t0 += ch) tasks.push_back(make_int2((int)(qi - q0), t0));
+        std::vector<int2> tasks;
+        w.slice_q.assign(1, 0);
+        w.slice_t.assign(1, 0);
+        const int ch = qx_der_chunk();
+        long long q0 = 0;
+        for (long long qi = 0; qi < w.nq; ++qi) {
+            if (qi - q0 == cap_q) {
+                q0 = qi;
+                w.slice_q.push_back(qi);
+                w.slice_t.push_back((long long)tasks.size());
+            }
+            const int np_q = h->pairs[list[qi].x].nprim * h->pairs[list[qi].y].nprim;
+            for (int t0 = 0; t0 < np_q; t0 += ch) tasks.push_back(make_int2((int)(qi - q0), t0));
+        }
+        w.slice_q.push_back(w.nq);
+        w.slice_t.push_back((long long)tasks.size());
+        if (cudaMalloc((void**)&w.d_dtasks, sizeof(int2) * tasks.size()) != cudaSuccess) {
+            cudaGetLastError();
+            w.d_dtasks = nullptr;
+            return fail(QX_E_NOMEM, "split-mode tasks for class %d", c);
+        }
+        w.ndtask = (long long)tasks.size();
+        QX_CUDA(cudaMemcpy(w.d_dtasks, tasks.data(), sizeof(int2) * tasks.size(), cudaMemcpyHostToDevice));
+        // a pageable host-to-device copy may still be in flight when cudaMemcpy
+        // returns, and the kernels that read the tasks run on non-blocking streams
+        QX_CUDA(cudaDeviceSynchronize());
     }
-    w.slice_q.push_back(w.nq);
-    w.slice_t.push_back((long long)tasks.size());
-    if (cudaMalloc((void**)&w.d_dtasks, sizeof(int2) * tasks.size()) != cudaSuccess ||
+    if (need_dacc && !w.d_dacc &&
         cudaMalloc((void**)&w.d_dacc, sizeof(double) * std::min(w.nq, cap_q) * nacc) != cudaSuccess) {
         cudaGetLastError();
-        cudaFree(w.d_dtasks);
-        w.d_dtasks = nullptr;
-        return fail(QX_E_NOMEM, "split-mode buffers for class %d", c);
+        w.d_dacc = nullptr;
+        return fail(QX_E_NOMEM, "split-mode derivative accumulators for class %d", c);
     }
-    w.ndtask = (long long)tasks.size();
-    QX_CUDA(cudaMemcpy(w.d_dtasks, tasks.data(), sizeof(int2) * tasks.size(), cudaMemcpyHostToDevice));
     return QX_OK;
 }
 
@@ -652,6 +668,13 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
             cudaMemcpy(w.d_q, sorted.data(), sizeof(int2) * w.nq, cudaMemcpyHostToDevice);
             w.d_q_full = w.d_q;
             w.nq_full = w.nq;
+            if (h->plain_eng[c] == ENG_WSPLIT) {
+                int rc = ensure_split_tasks(h, c, false, sorted.data());
+                if (rc) {
+                    free_handle(h);
+                    return rc;
+                }
+            }
             if (g_class_scratch[c] && h->plain_eng[c] == ENG_SL)
                 QX_ALLOC(w.scratch, sizeof(double) * g_class_scratch[c] * launch_threads(w.nq, w.log2g));
         }
@@ -936,7 +959,7 @@ static int run_deriv_class(qx_handle* h, int c, int mode, double* out, const dou
         // split modes, slice by slice: warp-program VRR into global accumulators
         // (ENG_WVRR) or the cooperative VRR, then the cooperative HRR pass
         if (g_der_idx[c] < 0) return fail(QX_E_UNSUPPORTED, "no derivative program for class %d", c);
-        int rc = ensure_split_tasks(h, c);
+        int rc = ensure_split_tasks(h, c, true);
         if (rc) return rc;
         const ClassWork& w = h->work[c];
         const long long nacc = qx_der_nacc(g_der_idx[c]);
@@ -1170,6 +1193,7 @@ extern "C" int qx_set_charges(qx_handle* h, const double* Z) {
     }
     QX_CUDA(cudaMemcpy(h->d_Z, Z, sizeof(double) * h->natom, cudaMemcpyHostToDevice));
     QX_CUDA(cudaMemcpy(h->d_xyz, h->coords.data(), sizeof(double) * 3 * h->natom, cudaMemcpyHostToDevice));
+    QX_CUDA(cudaDeviceSynchronize());  // the copies complete before any stream reads them
     return QX_OK;
 }
 

@@ -124,6 +124,9 @@ int setup_device(int dev) {
         return nofail(QX_E_CUDA, "qx_compute_2e_int_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
     const auto& tab = boys_host();
     e = cudaMemcpy(ptr, tab.data(), kBoysBytes, cudaMemcpyHostToDevice);
+    // a pageable host-to-device copy can still be in flight when cudaMemcpy returns;
+    // the caller's stream may not order after it, so wait here (set-up only)
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess)
         return nofail(QX_E_CUDA, "qx_compute_2e_int_noalloc: Boys table upload failed: %s", cudaGetErrorString(e));
     st.base = (unsigned char*)ptr;
