@@ -43,3 +43,21 @@ def test_rhf_gradient_against_finite_differences():
             Es.append(_scf(Molecule(mol.Z, c)).energy)
         fd = (Es[0] - Es[1]) / (2 * h)
         assert abs(g[nu] - fd) < 1e-6, (nu, g[nu], fd)
+
+
+def test_rhf_energies_against_published_values():
+    """Szabo & Ostlund, Modern Quantum Chemistry: STO-3G RHF total energies of H2 at
+    R = 1.4 bohr (-1.1167 Eh, sec. 3.5.2) and of H2O at R(OH) = 1.809 bohr,
+    104.52 degrees (-74.963 Eh, Table 3.13); compared to the digits quoted."""
+    import math
+
+    from quax_b200.methods.hartree_fock import restricted_hartree_fock
+
+    h2 = Molecule(np.array([1, 1]), np.array([[0.0, 0.0, 0.0], [0.0, 0.0, 1.4]]))
+    E = restricted_hartree_fock(h2, build_basis(h2, "sto-3g"), conv=1e-11).energy
+    assert abs(E - (-1.1167)) < 1e-4
+    R, th = 1.809, math.radians(104.52)
+    h2o = Molecule(np.array([8, 1, 1]),
+                   np.array([[0.0, 0.0, 0.0], [R, 0.0, 0.0], [R * math.cos(th), R * math.sin(th), 0.0]]))
+    E = restricted_hartree_fock(h2o, build_basis(h2o, "sto-3g"), conv=1e-11).energy
+    assert abs(E - (-74.963)) < 1e-3
