@@ -301,10 +301,88 @@ __global__ void __launch_bounds__(WARP_QPB * 32) k_warp(WarpArgs wa, int mode) {
             for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
             if (lane == 0) a.out[pq.x] = mx;
         } else if (mode == MODE_JK) {
-            for (int o = lane; o < W::NOUT; o += 32) {
-                const int id = o % ND, ic = (o / ND) % NC, ib = (o / (ND * NC)) % NB, ia = o / (ND * NC * NB);
-                jk_images(a.out, a.out2, a.dens, n, P.bf1 + ia, P.bf2 + ib, Q.bf1 + ic, Q.bf2 + id, s12, s34, sPQ,
-                          H[__ldg(outs + o)]);
+            // J/K from the whole quartet block at once: the up-to-8 images of each
+            // integral regroup into six block contractions with D (JA = G.D_CD over
+            // the ket, JC = D_AB.G over the bra, and the four exchange blocks), so
+            // each touched J/K entry takes one atomic per quartet instead of one per
+            // integral and image.
+            constexpr int NA = ncart_h(W::LA);
+            const double* __restrict__ Dm = a.dens;
+            double* __restrict__ Jm = a.out;
+            double* __restrict__ Km = a.out2;
+            const long long bA = P.bf1, bB = P.bf2, bC = Q.bf1, bD = Q.bf2;
+            auto G = [&](int ia, int ib, int ic, int id) {
+                return H[__ldg(outs + ((ia * NB + ib) * NC + ic) * ND + id)];
+            };
+            auto Dv = [&](long long r, long long c) { return __ldg(Dm + r * n + c); };
+            constexpr int nJA = NA * NB, nJC = NC * ND, nK1 = NA * NC, nK2 = NB * NC, nK3 = NA * ND, nK4 = NB * ND;
+            constexpr int total = nJA + nJC + nK1 + nK2 + nK3 + nK4;
+            for (int e = lane; e < total; e += 32) {
+                int r = e;
+                if (r < nJA) {  // J_ij += (1 + s34) sum_kl G D_kl, and J_ji with s12
+                    const int ia = r / NB, ib = r % NB;
+                    double x = 0.0;
+                    for (int ic = 0; ic < NC; ++ic)
+                        for (int id = 0; id < ND; ++id) x = fma(G(ia, ib, ic, id), Dv(bC + ic, bD + id), x);
+                    x *= 1.0 + s34;
+                    atomicAdd(Jm + (bA + ia) * n + bB + ib, x);
+                    if (s12) atomicAdd(Jm + (bB + ib) * n + bA + ia, x);
+                    continue;
+                }
+                r -= nJA;
+                if (r < nJC) {  // with sPQ: J_kl += (1 + s12) sum_ij G D_ij, and J_lk with s34
+                    if (!sPQ) continue;
+                    const int ic = r / ND, id = r % ND;
+                    double x = 0.0;
+                    for (int ia = 0; ia < NA; ++ia)
+                        for (int ib = 0; ib < NB; ++ib) x = fma(G(ia, ib, ic, id), Dv(bA + ia, bB + ib), x);
+                    x *= 1.0 + s12;
+                    atomicAdd(Jm + (bC + ic) * n + bD + id, x);
+                    if (s34) atomicAdd(Jm + (bD + id) * n + bC + ic, x);
+                    continue;
+                }
+                r -= nJC;
+                if (r < nK1) {  // K_ik += sum_jl G D_jl (and K_ki with sPQ)
+                    const int ia = r / NC, ic = r % NC;
+                    double x = 0.0;
+                    for (int ib = 0; ib < NB; ++ib)
+                        for (int id = 0; id < ND; ++id) x = fma(G(ia, ib, ic, id), Dv(bB + ib, bD + id), x);
+                    atomicAdd(Km + (bA + ia) * n + bC + ic, x);
+                    if (sPQ) atomicAdd(Km + (bC + ic) * n + bA + ia, x);
+                    continue;
+                }
+                r -= nK1;
+                if (r < nK2) {  // with s12: K_jk += sum_il G D_il (and K_kj with sPQ)
+                    if (!s12) continue;
+                    const int ib = r / NC, ic = r % NC;
+                    double x = 0.0;
+                    for (int ia = 0; ia < NA; ++ia)
+                        for (int id = 0; id < ND; ++id) x = fma(G(ia, ib, ic, id), Dv(bA + ia, bD + id), x);
+                    atomicAdd(Km + (bB + ib) * n + bC + ic, x);
+                    if (sPQ) atomicAdd(Km + (bC + ic) * n + bB + ib, x);
+                    continue;
+                }
+                r -= nK2;
+                if (r < nK3) {  // with s34: K_il += sum_jk G D_jk (and K_li with sPQ)
+                    if (!s34) continue;
+                    const int ia = r / ND, id = r % ND;
+                    double x = 0.0;
+                    for (int ib = 0; ib < NB; ++ib)
+                        for (int ic = 0; ic < NC; ++ic) x = fma(G(ia, ib, ic, id), Dv(bB + ib, bC + ic), x);
+                    atomicAdd(Km + (bA + ia) * n + bD + id, x);
+                    if (sPQ) atomicAdd(Km + (bD + id) * n + bA + ia, x);
+                    continue;
+                }
+                r -= nK3;
+                {  // with s12 and s34: K_jl += sum_ik G D_ik (and K_lj with sPQ)
+                    if (!(s12 && s34)) continue;
+                    const int ib = r / ND, id = r % ND;
+                    double x = 0.0;
+                    for (int ia = 0; ia < NA; ++ia)
+                        for (int ic = 0; ic < NC; ++ic) x = fma(G(ia, ib, ic, id), Dv(bA + ia, bC + ic), x);
+                    atomicAdd(Km + (bB + ib) * n + bD + id, x);
+                    if (sPQ) atomicAdd(Km + (bD + id) * n + bB + ib, x);
+                }
             }
         } else {
             for (int o = lane; o < W::NOUT; o += 32) {
