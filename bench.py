@@ -437,7 +437,9 @@ def gradient_30_atoms():
 def batched_extras(count: int, iterations: int = 20):
     """Batched RHF: `count` Gaussian-displaced geometries (sigma 0.05 bohr) of one
     12-atom synthetic molecule, J/K of the whole batch replayed from one CUDA graph
-    per SCF iteration, then the analytic gradients."""
+    per SCF iteration (incremental builds from the density change with density
+    screening at 1e-12, full rebuild every 8 iterations), then the analytic
+    gradients."""
     import torch
 
     from quax_b200.basis import SyntheticSpec, synthetic_molecule
@@ -448,7 +450,7 @@ def batched_extras(count: int, iterations: int = 20):
     mols = displaced_geometries(mol0, count, 0.05, seed=1)
     bases = [b0.with_coords(m.coords) for m in mols]
     t0 = time.perf_counter()
-    br = BatchedRHF(mols, bases, ints_tol=THR)
+    br = BatchedRHF(mols, bases, ints_tol=THR, incremental=1e-12, rebuild_every=8)
     nq = sum(m.eng.unique_quartets() for m in br.mols)
     # eager J/K of the batch, for comparison with the graph replay
     br._jk_all()

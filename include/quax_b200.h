@@ -150,6 +150,15 @@ int qx_class_info(const qx_handle *h, int cls, int *l4, long long *nquartets, lo
 int qx_grad_adjoint_jvp(qx_handle *h, const double *D, double cj, double ck, const double *v, double *Hv,
                         int on_device, void *stream);
 
+/* Direct J/K with density screening, no counterpart in the reference: like
+ * qx_jk (device pointers only) but a quartet is skipped when
+ * sqrt(K_ab) sqrt(K_cd) max|D| over its six shell-pair blocks < thr, which bounds
+ * every J/K contribution it could make (Schwarz inequality).  With the density
+ * change of an SCF iteration as D (incremental Fock builds) most quartets drop
+ * out as the SCF converges.  The first call uploads per-pair bounds
+ * (synchronises); later calls allocate nothing. */
+int qx_jk_screened(qx_handle *h, const double *D, double *J, double *K, double thr, void *stream);
+
 /* One-electron integrals (the reference's compute_1e_int("overlap"|"kinetic"|
  * "potential"), libint_interface.cc:232-483, and oei_deriv_core(1), :2403-2579),
  * on the device, Cartesian, same conventions as the two-electron integrals.

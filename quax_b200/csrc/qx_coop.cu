@@ -65,6 +65,7 @@ __global__ void __launch_bounds__(COOP_WPB * 32) k_coop(CoopArgs ca, int mode) {
     const int2 pq = a.quartets[qi];
     const PairInfo P = a.pairs[pq.x];
     const PairInfo Q = a.pairs[pq.y];
+    if (mode == MODE_JK && jk_screened(a, pq, P, Q)) return;  // whole block, before any barrier
     const uint4* __restrict__ vn = g_coop_vnodes + C.vnode_off;
     const int* __restrict__ vl = g_coop_vlev + C.vlev_off;
     const unsigned short* __restrict__ tg = g_coop_targets + C.tgt_off;

@@ -265,6 +265,11 @@ struct qx_handle {
     int wpq[QX_NUM_CLASSES];        // warps per quartet, plain warp kernels
     int wpq_deriv[QX_NUM_CLASSES];  // warps per quartet, derivative warp kernels
     int shard_rank = 0, shard_n = 1;
+    // J/K density screening: sqrt(K) and max |D| per pair record, threshold of the
+    // call in progress (0 = off)
+    double* d_kpair = nullptr;
+    double* d_dmax = nullptr;
+    double jk_thr = 0.0;
     // one-electron integrals: nuclear charges and positions on the device
     double* d_Z = nullptr;
     double* d_xyz = nullptr;
@@ -390,6 +395,8 @@ static void free_handle(qx_handle* h) {
     if (h->start) cudaEventDestroy(h->start);
     cudaFree(h->d_Z);
     cudaFree(h->d_xyz);
+    cudaFree(h->d_kpair);
+    cudaFree(h->d_dmax);
     delete h;
 }
 
@@ -418,6 +425,11 @@ static int run_class(qx_handle* h, int cls, int mode, const int2* d_q, long long
     a.log2g = eng == ENG_SL ? log2g : 0;
     a.err = h->d_err;
     if (d_q == h->work[cls].d_q) a.nq64 = h->work[cls].nq64;
+    if (mode == MODE_JK && h->jk_thr > 0.0) {
+        a.jk_thr = h->jk_thr;
+        a.jk_kpair = h->d_kpair;
+        a.jk_dmax = h->d_dmax;
+    }
     if (eng == ENG_COOP) {
         qx_launch_coop(g_coop_idx[cls], a, mode, s);
     } else if (eng == ENG_WARP || eng == ENG_WSPLIT) {
@@ -1397,6 +1409,53 @@ extern "C" int qx_engine_config(const qx_handle* h, int cls, int* cfg) {
 }
 
 // ---------------------------------------------------------------- direct J/K ---
+// max |D| over each pair record's block (one warp per pair record)
+__global__ void __launch_bounds__(128) k_pair_dmax(const PairInfo* __restrict__ pairs, int npair,
+                                                   const double* __restrict__ D, long long n, double* __restrict__ out) {
+    const int p = blockIdx.x * 4 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (p >= npair) return;
+    const PairInfo P = pairs[p];
+    const int na = (P.l1 + 1) * (P.l1 + 2) / 2, nb = (P.l2 + 1) * (P.l2 + 2) / 2;
+    double m = 0.0;
+    for (int e = lane; e < na * nb; e += 32) {
+        const long long i = P.bf1 + e / nb, j = P.bf2 + e % nb;
+        m = fmax(m, fmax(fabs(D[i * n + j]), fabs(D[j * n + i])));
+    }
+    for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, off));
+    if (lane == 0) out[p] = m;
+}
+
+extern "C" int qx_jk_screened(qx_handle* h, const double* D, double* J, double* K, double thr, void* stream) {
+    if (!h || !D || !J || !K) return fail(QX_E_INVALID, "qx_jk_screened: NULL argument");
+    if (!(thr >= 0.0) || !std::isfinite(thr)) return fail(QX_E_INVALID, "qx_jk_screened: bad threshold");
+    DeviceGuard g(h->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const int np = (int)h->pairs.size();
+    if (!h->d_kpair) {  // first call: per-pair sqrt(K) (host data) and the max |D| buffer
+        std::vector<double> kp(np);
+        for (int p = 0; p < np; ++p)
+            kp[p] = std::sqrt(h->K[(size_t)h->pairs[p].s1 * h->nshell + h->pairs[p].s2]);
+        if (cudaMalloc((void**)&h->d_kpair, sizeof(double) * np) != cudaSuccess ||
+            cudaMalloc((void**)&h->d_dmax, sizeof(double) * np) != cudaSuccess) {
+            cudaGetLastError();
+            cudaFree(h->d_kpair);
+            h->d_kpair = nullptr;
+            return fail(QX_E_NOMEM, "qx_jk_screened: allocation failed");
+        }
+        QX_CUDA(cudaMemcpy(h->d_kpair, kp.data(), sizeof(double) * np, cudaMemcpyHostToDevice));
+        QX_CUDA(cudaDeviceSynchronize());  // the copy completes before any stream reads it
+    }
+    const long long n = h->nbf;
+    QX_CUDA(cudaMemsetAsync(J, 0, sizeof(double) * n * n, s));
+    QX_CUDA(cudaMemsetAsync(K, 0, sizeof(double) * n * n, s));
+    k_pair_dmax<<<(np + 3) / 4, 128, 0, s>>>(h->d_pairs, np, D, n, h->d_dmax);
+    QX_CUDA(cudaGetLastError());
+    h->jk_thr = thr;
+    int rc = run_all_classes(h, MODE_JK, J, n, s, K, D);
+    h->jk_thr = 0.0;
+    return rc;
+}
+
 extern "C" int qx_jk(qx_handle* h, const double* D, double* J, double* K, int on_device, void* stream) {
     if (!h || !D || !J || !K) return fail(QX_E_INVALID, "qx_jk: NULL argument");
     DeviceGuard g(h->device);

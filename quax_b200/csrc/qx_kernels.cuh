@@ -28,7 +28,24 @@ struct EriArgs {
     // mixed precision: quartets [nq64, nq) of the list run their recurrences in
     // FP32 (warp and split engines); the default keeps every quartet FP64
     long long nq64 = 0x7fffffffffffffffLL;
+    // density screening of J/K (MODE_JK): a quartet is skipped when
+    // sqrt(K_ab) sqrt(K_cd) max(|D| over its six shell-pair blocks) < jk_thr
+    const double* jk_kpair = nullptr;  // sqrt(Schwarz K) per pair record
+    const double* jk_dmax = nullptr;   // max |D| per pair record
+    double jk_thr = 0.0;
 };
+
+// True when density screening drops this quartet from J/K.
+__device__ __forceinline__ bool jk_screened(const EriArgs& a, int2 pq, const PairInfo& P, const PairInfo& Q) {
+    if (!a.jk_dmax) return false;
+    auto pidx = [](int s, int t) { return s >= t ? s * (s + 1) / 2 + t : t * (t + 1) / 2 + s; };
+    double dm = fmax(__ldg(a.jk_dmax + pq.x), __ldg(a.jk_dmax + pq.y));
+    dm = fmax(dm, __ldg(a.jk_dmax + pidx(P.s1, Q.s1)));
+    dm = fmax(dm, __ldg(a.jk_dmax + pidx(P.s2, Q.s2)));
+    dm = fmax(dm, __ldg(a.jk_dmax + pidx(P.s1, Q.s2)));
+    dm = fmax(dm, __ldg(a.jk_dmax + pidx(P.s2, Q.s1)));
+    return __ldg(a.jk_kpair + pq.x) * __ldg(a.jk_kpair + pq.y) * dm < a.jk_thr;
+}
 
 // Accumulator storage for the contracted [e0|f0] targets of one quartet.
 template <int N>
@@ -190,11 +207,12 @@ __global__ void __launch_bounds__(AccPolicy<EriCls<LA, LB, LC, LD>::NACC>::bs) k
     const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long qi = gt >> a.log2g;
     const int sub = (int)(gt & ((1 << a.log2g) - 1));
-    const bool active = qi < a.nq;
+    bool active = qi < a.nq;
     // every lane stays to the end: the group reduction shuffles over the full warp
     const int2 pq = active ? a.quartets[qi] : make_int2(0, 0);
     const PairInfo P = a.pairs[pq.x];
     const PairInfo Q = a.pairs[pq.y];
+    if (MODE == MODE_JK && active && jk_screened(a, pq, P, Q)) active = false;  // group-uniform
     if constexpr (Pol::kind == ACC_REG) {
         RegAcc<C::NACC> acc;
         contract_quartet<C>(a, P, Q, acc, sub, active);

@@ -204,6 +204,8 @@ __global__ void __launch_bounds__(WARP_QPB * 32) k_warp(WarpArgs wa, int mode) {
     const PairInfo Q = a.pairs[pq.y];
     const int atA = P.atom1, atB = P.atom2, atC = Q.atom1, atD = Q.atom2;
     const bool f32 = qi >= a.nq64;  // warp-uniform: one quartet per warp
+    // density screening (J/K): the whole warp, or all warps of a wpq = 4 block
+    if (!DERIV && mode == MODE_JK && jk_screened(a, pq, P, Q)) return;
     if (DERIV) {
         if (atA == atB && atA == atC && atA == atD) return;  // reference skips these
         if (mode == WMODE_DER_SLICE) {
@@ -553,6 +555,7 @@ __global__ void __launch_bounds__(WARP_QPB * 32) k_gvrr(EriArgs a, const int2* _
     const PairInfo P = a.pairs[pq.x];
     const PairInfo Q = a.pairs[pq.y];
     if (DER && P.atom1 == P.atom2 && P.atom1 == Q.atom1 && P.atom1 == Q.atom2) return;  // reference skips these
+    if (!DER && jk_screened(a, pq, P, Q)) return;  // J/K density screening (set only in J/K calls)
     double* qacc = acc + (size_t)task.x * (DER ? nacc : W::NITEM_PAD);
     const bool f32 = task.x >= a.nq64;  // warp-uniform: one task per warp
     extern __shared__ double wv_sm[];

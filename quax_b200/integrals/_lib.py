@@ -55,6 +55,7 @@ SIGNATURES = {
     "qx_grad_adjoint_class": (C.c_int, [_vp, C.c_int, _vp, C.c_double, C.c_double, _vp, _vp]),
     "qx_autotune": (C.c_int, [_vp, C.c_int, _vp]),
     "qx_set_charges": (C.c_int, [_vp, _vp]),
+    "qx_jk_screened": (C.c_int, [_vp, _vp, _vp, _vp, C.c_double, _vp]),
     "qx_oei": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "qx_oei_deriv_core": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, _vp]),
     "qx_grad_adjoint_jvp": (C.c_int, [_vp, _vp, C.c_double, C.c_double, _vp, _vp, C.c_int, _vp]),

@@ -281,8 +281,11 @@ class EriEngine:
         return out
 
     # -- Fock-matrix pieces -----------------------------------------------------
-    def jk(self, D: torch.Tensor, J: torch.Tensor | None = None, K: torch.Tensor | None = None, stream=None):
-        """Direct J_ij = sum (ij|kl) D_kl and K_ij = sum (ik|jl) D_kl (D symmetric)."""
+    def jk(self, D: torch.Tensor, J: torch.Tensor | None = None, K: torch.Tensor | None = None, stream=None,
+           screen: float = 0.0):
+        """Direct J_ij = sum (ij|kl) D_kl and K_ij = sum (ik|jl) D_kl (D symmetric).
+        screen > 0 skips quartets whose Schwarz bound times the largest density block
+        they touch is below it (for incremental builds from a density change)."""
         D = D.to(device=self.device, dtype=torch.float64).contiguous()
         n = self.nbf
         if J is None:
@@ -290,9 +293,17 @@ class EriEngine:
         if K is None:
             K = torch.empty((n, n), dtype=torch.float64, device=self.device)
         with torch.cuda.device(self.device):
-            _lib.check(
-                _lib.load().qx_jk(self.handle, C.c_void_p(D.data_ptr()), C.c_void_p(J.data_ptr()),
-                                  C.c_void_p(K.data_ptr()), 1, C.c_void_p(_stream_ptr(stream))),
-                "qx_jk",
-            )
+            if screen > 0.0:
+                _lib.check(
+                    _lib.load().qx_jk_screened(self.handle, C.c_void_p(D.data_ptr()), C.c_void_p(J.data_ptr()),
+                                               C.c_void_p(K.data_ptr()), float(screen),
+                                               C.c_void_p(_stream_ptr(stream))),
+                    "qx_jk_screened",
+                )
+            else:
+                _lib.check(
+                    _lib.load().qx_jk(self.handle, C.c_void_p(D.data_ptr()), C.c_void_p(J.data_ptr()),
+                                      C.c_void_p(K.data_ptr()), 1, C.c_void_p(_stream_ptr(stream))),
+                    "qx_jk",
+                )
         return J, K

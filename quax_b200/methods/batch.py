@@ -40,6 +40,10 @@ class _Mol:
     D: torch.Tensor
     J: torch.Tensor
     K: torch.Tensor
+    dD: torch.Tensor = None  # incremental builds: density change and its J/K
+    Jd: torch.Tensor = None
+    Kd: torch.Tensor = None
+    Dold: torch.Tensor = None
     F: torch.Tensor = None
     C: torch.Tensor = None
     eps: torch.Tensor = None
@@ -49,7 +53,11 @@ class _Mol:
 
 
 class BatchedRHF:
-    def __init__(self, molecules, bases, ints_tol: float = 1.0e-12, streams: int = 8, autotune: bool = False):
+    def __init__(self, molecules, bases, ints_tol: float = 1.0e-12, streams: int = 8, autotune: bool = False,
+                 incremental: float = 0.0, rebuild_every: int = 8):
+        """incremental > 0: after the first iteration, J and K are updated from the
+        density change with density screening at that threshold (qx_jk_screened),
+        and rebuilt in full every `rebuild_every` iterations."""
         if len(molecules) != len(bases):
             raise ValueError("one basis per molecule")
         self.dev = torch.device("cuda")
@@ -65,39 +73,62 @@ class BatchedRHF:
             n = eng.nbf
             z = lambda: torch.zeros((n, n), dtype=torch.float64, device=self.dev)
             self.mols.append(_Mol(mol, b, eng, A, T + V, S, nuclear_repulsion(mol.Z, mol.coords),
-                                  mol.nelectron // 2, z(), z(), z()))
+                                  mol.nelectron // 2, z(), z(), z(), z(), z(), z(), z()))
         torch.cuda.synchronize()
         self.setup_s = time.perf_counter() - t0
         self.side = [torch.cuda.Stream(device=self.dev) for _ in range(streams)]
         self.graph = None
+        self.graph_inc = None
+        self.incremental = incremental
+        self.rebuild_every = rebuild_every
 
     # -- J/K of the whole batch ---------------------------------------------------
-    def _jk_all(self):
+    def _jk_all(self, inc: bool = False):
         cur = torch.cuda.current_stream()
         used = self.side[: min(len(self.side), len(self.mols))]
         for s in used:  # fork every used side stream from the current one (joins the capture)
             s.wait_stream(cur)
         for k, m in enumerate(self.mols):
-            m.eng.jk(m.D, m.J, m.K, stream=used[k % len(used)])
+            if inc:
+                m.eng.jk(m.dD, m.Jd, m.Kd, stream=used[k % len(used)], screen=self.incremental)
+            else:
+                m.eng.jk(m.D, m.J, m.K, stream=used[k % len(used)])
         for s in used:
             cur.wait_stream(s)
 
     def capture(self):
-        """Record the batch's J/K builds into one CUDA graph (after a warm-up run that
-        makes every lazy allocation of the handles)."""
-        self._jk_all()
-        torch.cuda.synchronize()
-        g = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(g):
-            self._jk_all()
-        torch.cuda.synchronize()
-        self.graph = g
+        """Record the batch's J/K builds into CUDA graphs (after a warm-up run that
+        makes every lazy allocation of the handles): the full build from D, and with
+        incremental builds the screened build from the density change."""
+        for inc in ((False, True) if self.incremental > 0 else (False,)):
+            self._jk_all(inc)
+            torch.cuda.synchronize()
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                self._jk_all(inc)
+            torch.cuda.synchronize()
+            if inc:
+                self.graph_inc = g
+            else:
+                self.graph = g
 
-    def jk(self):
-        if self.graph is not None:
+    def jk(self, inc: bool = False):
+        if inc:
+            for m in self.mols:
+                torch.sub(m.D, m.Dold, out=m.dD)
+            if self.graph_inc is not None:
+                self.graph_inc.replay()
+            else:
+                self._jk_all(True)
+            for m in self.mols:
+                m.J += m.Jd
+                m.K += m.Kd
+        elif self.graph is not None:
             self.graph.replay()
         else:
             self._jk_all()
+        for m in self.mols:
+            m.Dold.copy_(m.D)
 
     # -- SCF -------------------------------------------------------------------
     def _diag(self, m: _Mol, F: torch.Tensor):
@@ -115,8 +146,9 @@ class BatchedRHF:
         t_jk = 0.0
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         for it in range(iterations):
+            inc = self.incremental > 0 and it % self.rebuild_every != 0
             e0.record()
-            self.jk()
+            self.jk(inc)
             e1.record()
             torch.cuda.synchronize()
             t_jk += e0.elapsed_time(e1) * 1e-3
@@ -171,6 +203,7 @@ class BatchedRHF:
 
     def close(self):
         self.graph = None
+        self.graph_inc = None
         for m in self.mols:
             m.eng.close()
 

@@ -52,3 +52,16 @@ def test_graph_replay_equals_eager():
     assert np.abs(np.array(Ea) - np.array(Eb)).max() < 1e-12
     a.close()
     b.close()
+
+
+def test_incremental_screened_scf_matches_full_builds():
+    from quax_b200.methods.batch import BatchedRHF
+
+    mols, bases = _batch()
+    full = BatchedRHF(mols, bases, ints_tol=1e-12)
+    Ef, _ = full.scf(iterations=30, use_graph=True)
+    inc = BatchedRHF(mols, bases, ints_tol=1e-12, incremental=1e-12, rebuild_every=8)
+    Ei, _ = inc.scf(iterations=30, use_graph=True)
+    assert np.abs(np.array(Ef) - np.array(Ei)).max() < 1e-8
+    full.close()
+    inc.close()
