@@ -1,0 +1,51 @@
+"""Edge cases of the ERI path against the oracle (GPU): a single shell on one atom
+(one quartet per class), atoms 30 bohr apart (Boys arguments far beyond the
+tabulated range, asymptotic branch), exponents from 0.01 to 1e5 (T near 0 and
+huge prefactors), a loose threshold that screens most quartets, and the unique
+quartet counts.  Tolerance 1e-12 absolute (relative for values above 1)."""
+import numpy as np
+import pytest
+
+from quax_b200.basis import Basis, Shell
+
+pytestmark = pytest.mark.gpu
+
+
+def _check(oracle_lib, b, tol):
+    from quax_b200.integrals.engine import EriEngine
+
+    eng = EriEngine(b, tol)
+    ob = oracle_lib.OracleBasis(b)
+    G = eng.eri().cpu().numpy()
+    ref = oracle_lib.compute_2e_int(ob, tol)
+    assert np.abs(G - ref).max() < 1e-12 * max(1.0, np.abs(ref).max())
+    assert eng.unique_quartets() == oracle_lib.count_unique(ob, tol)
+    eng.close()
+    return eng
+
+
+@pytest.mark.parametrize("l", [0, 1, 2])
+def test_single_shell(oracle_lib, l):
+    b = Basis([Shell(l, np.array([1.7, 0.3]), np.array([0.4, 0.7]), np.zeros(3), 0)], 1, False, "edge")
+    _check(oracle_lib, b, 1e-14)
+
+
+def test_far_apart_and_extreme_exponents(oracle_lib):
+    shells = [
+        Shell(0, np.array([1.0e5, 3.0e3, 90.0]), np.array([0.2, 0.5, 0.6]), np.zeros(3), 0),
+        Shell(1, np.array([0.01]), np.array([1.0]), np.zeros(3), 0),
+        Shell(2, np.array([4.0, 0.05]), np.array([0.5, 0.5]), np.array([0.0, 0.0, 30.0]), 1),
+        Shell(1, np.array([2.5e4, 7.0]), np.array([0.3, 0.8]), np.array([0.0, 0.0, 30.0]), 1),
+    ]
+    _check(oracle_lib, Basis(shells, 2, False, "edge"), 1e-14)
+
+
+def test_loose_threshold_screens_most_quartets(oracle_lib):
+    from quax_b200.basis import SyntheticSpec, synthetic_molecule
+
+    spec = SyntheticSpec(natom=4, box=12.0, min_sep=3.0, kmax=3, exp_lo=0.5, exp_hi=50.0)
+    b = synthetic_molecule(spec, 2)[1]
+    loose = oracle_lib.count_unique(oracle_lib.OracleBasis(b), 1e-4)
+    tight = oracle_lib.count_unique(oracle_lib.OracleBasis(b), 1e-14)
+    assert loose < tight
+    _check(oracle_lib, b, 1e-4)
