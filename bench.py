@@ -198,7 +198,10 @@ def run_ours(args):
         ms = float(t.item())
     ms_per_step = ms / args.steps
     value = world * nq / (ms_per_step * 1e-3)
-    launches = sum(1 for c in info if c["nq"] > 0) * args.steps
+    # our kernels per step: one per class with quartets, two for split-mode classes
+    # (primitive-chunk VRR + HRR)
+    cfg = eng.engine_config()
+    launches = sum(2 if cfg["%d%d%d%d" % c["l"]][0] == "wsplit" else 1 for c in info if c["nq"] > 0) * args.steps
 
     if args.no_extras:
         torch.cuda.profiler.stop()
