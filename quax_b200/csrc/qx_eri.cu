@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <functional>
 #include <cmath>
 #include <cstdarg>
@@ -283,7 +284,8 @@ struct qx_handle {
 // most QX_SPLIT_ACC_BYTES of derivative accumulators; each slice runs as its own
 // VRR + HRR pair.  `list` is the class's current view when the caller has it on
 // the host (set-up), else it is copied back from the device.
-static int ensure_split_tasks(qx_handle* h, int c, bool need_dacc = false, const int2* list = nullptr) {
+static int ensure_split_tasks(qx_handle* h, int c, bool need_dacc = false, const int2* list = nullptr,
+                              bool sync = true) {
     ClassWork& w = h->work[c];
     if (!w.nq) return QX_OK;
     const long long nacc = qx_der_nacc(g_der_idx[c]);
@@ -320,7 +322,8 @@ static int ensure_split_tasks(qx_handle* h, int c, bool need_dacc = false, const
         QX_CUDA(cudaMemcpy(w.d_dtasks, tasks.data(), sizeof(int2) * tasks.size(), cudaMemcpyHostToDevice));
         // a pageable host-to-device copy may still be in flight when cudaMemcpy
         // returns, and the kernels that read the tasks run on non-blocking streams
-        QX_CUDA(cudaDeviceSynchronize());
+        // (set-up synchronises once at its end instead)
+        if (sync) QX_CUDA(cudaDeviceSynchronize());
     }
     if (need_dacc && !w.d_dacc &&
         cudaMalloc((void**)&w.d_dacc, sizeof(double) * std::min(w.nq, cap_q) * nacc) != cudaSuccess) {
@@ -464,6 +467,21 @@ static int run_class(qx_handle* h, int cls, int mode, const int2* d_q, long long
     return QX_OK;
 }
 
+// QX_TRACE_INIT=1 prints the set-up phases' wall times to stderr (diagnostics).
+namespace {
+struct InitTrace {
+    bool on = std::getenv("QX_TRACE_INIT") != nullptr;
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    void mark(const char* what) {
+        if (!on) return;
+        const auto t1 = std::chrono::steady_clock::now();
+        std::fprintf(stderr, "qx_initialize: %-28s %8.3f ms\n", what,
+                     std::chrono::duration<double, std::milli>(t1 - t0).count());
+        t0 = t1;
+    }
+};
+}  // namespace
+
 extern "C" int qx_initialize(int natom, const double* coords, int nshell, const int* shell_l, const int* shell_nprim,
                              const int* shell_atom, const double* exps, const double* coefs, int pure,
                              double ints_tol, qx_handle** out) {
@@ -475,6 +493,7 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
     if (!(ints_tol > 0.0) || !std::isfinite(ints_tol)) return fail(QX_E_INVALID, "qx_initialize: ints_tol must be > 0");
     for (int i = 0; i < 3 * natom; ++i)
         if (!std::isfinite(coords[i])) return fail(QX_E_INVALID, "qx_initialize: non-finite coordinate %d", i);
+    InitTrace trace;
     qx_handle* h = new qx_handle();
     cudaGetDevice(&h->device);
     choose_engines(h);
@@ -532,6 +551,7 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
         bf += ncart_h(l);
     }
     h->nbf = bf;
+    trace.mark("shells");
     // pair records
     std::vector<PrimPair> prims;
     const double kfac = std::sqrt(2.0) * std::pow(M_PI, 1.25);
@@ -610,8 +630,14 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
         for (int pc = 0; pc < QX_NUM_PAIR_CLASSES; ++pc) {
             if (diag[pc].empty()) continue;
             cudaMemcpy(d_dq + o, diag[pc].data(), sizeof(int2) * diag[pc].size(), cudaMemcpyHostToDevice);
-            int rc = run_class(h, quartet_class(pc, pc), MODE_SCHWARZ, d_dq + o, (long long)diag[pc].size(), d_kp, 0,
-                               0, 0);
+            // few quartets with long primitive loops: 32 lanes (straight-line kernels
+            // without global accumulators) or 4 warps (warp kernels) per quartet
+            const int cls = quartet_class(pc, pc);
+            const int keep_wpq = h->wpq[cls];
+            h->wpq[cls] = 4;
+            int rc = run_class(h, cls, MODE_SCHWARZ, d_dq + o, (long long)diag[pc].size(), d_kp, 0, 0, 0,
+                               g_class_scratch[cls] ? 0 : 5);
+            h->wpq[cls] = keep_wpq;
             if (rc) { cudaFree(d_kp); cudaFree(d_dq); free_handle(h); return rc; }
             o += diag[pc].size();
         }
@@ -630,6 +656,7 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
             h->kmax = std::max(h->kmax, kp[p]);
         }
     }
+    trace.mark("pairs, uploads, Schwarz");
     // screened pair list (reference order s1 >= s2) and unique quartets
     const double thr2 = ints_tol * ints_tol;
     const double cut = thr2 / h->kmax;
@@ -681,7 +708,7 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
             w.d_q_full = w.d_q;
             w.nq_full = w.nq;
             if (h->plain_eng[c] == ENG_WSPLIT) {
-                int rc = ensure_split_tasks(h, c, false, sorted.data());
+                int rc = ensure_split_tasks(h, c, false, sorted.data(), false);
                 if (rc) {
                     free_handle(h);
                     return rc;
@@ -692,6 +719,7 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
         }
     }
     h->unique_size = base;
+    trace.mark("quartet lists, split tasks");
     for (int c = 0; c < QX_NUM_CLASSES; ++c) h->order[c] = c;
     std::sort(h->order, h->order + QX_NUM_CLASSES,
               [&](int x, int y) { return h->work[x].prims * g_class_nout[x] > h->work[y].prims * g_class_nout[y]; });
@@ -712,6 +740,7 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
         free_handle(h);
         return fail(QX_E_CUDA, "qx_initialize: %s", cudaGetErrorString(e));
     }
+    trace.mark("streams, final sync");
     *out = h;
     return QX_OK;
 }
