@@ -137,8 +137,84 @@ def generate_multi_index_lookup(nparams: int, deriv_order: int):
     return _lookup(nparams, deriv_order)
 
 
-def compute_2e_deriv_disk(type_: str, beta: float, max_deriv_order: int):
-    raise NotImplementedError("HDF5 disk mode (libint_interface.cc:1811-2115) is not part of this build")
+# -- disk format (libint_interface.cc:1338-1567, 1811-2115; read by tei.py:157-181) ----
+# The reference writes HDF5 files with one dataset per derivative order, named
+# <type>_<nbf...>_deriv<k> and shaped (nbf..., nderiv) -- the derivative index last.
+# h5py is optional here: with it the same .h5 files are written; without it the
+# same datasets go to a NumPy archive of the same stem (.npz).
+_DISK_LIMIT_GB = 50.0  # the reference asserts the same bound (libint_interface.cc:1819)
+
+
+def _write_datasets(stem: str, datasets: dict) -> str:
+    try:
+        import h5py
+    except ImportError:
+        h5py = None
+    if h5py is not None:
+        path = stem + ".h5"
+        with h5py.File(path, "w") as f:
+            for k, v in datasets.items():
+                f.create_dataset(k, data=v)
+    else:
+        path = stem + ".npz"
+        np.savez(path, **datasets)
+    return path
+
+
+def read_dataset(stem: str, name: str) -> np.ndarray:
+    """One dataset of a file written by the *_deriv_disk functions (.h5 or .npz)."""
+    import os
+
+    if os.path.exists(stem + ".h5"):
+        import h5py
+
+        with h5py.File(stem + ".h5", "r") as f:
+            return f[name][()]
+    if os.path.exists(stem + ".npz"):
+        with np.load(stem + ".npz") as z:
+            return z[name]
+    raise FileNotFoundError(f"{stem}.h5 / {stem}.npz not found")
+
+
+def compute_2e_deriv_disk(type_: str, beta: float, max_deriv_order: int) -> str:
+    """Write every ERI derivative tensor up to max_deriv_order to eri_derivs.(h5|npz):
+    datasets eri_<n>_<n>_<n>_<n>_deriv<k>, shape (n, n, n, n, nderiv)."""
+    _check_type(type_)
+    eng = _engine()
+    n = eng.nbf
+    slices = sum(how_many_derivs(eng.natom, k) for k in range(1, max_deriv_order + 1))
+    if n**4 * slices * 8e-9 >= _DISK_LIMIT_GB:
+        raise ValueError(f"ERI derivative tensors need {n**4 * slices * 8e-9:.0f} GB (limit {_DISK_LIMIT_GB:.0f} GB)")
+    if max_deriv_order > LIBINT2_MAX_DERIV_ORDER:
+        raise NotImplementedError(f"derivative order {max_deriv_order} (this build: {LIBINT2_MAX_DERIV_ORDER})")
+    data = {}
+    for k in range(1, max_deriv_order + 1):
+        d = eng.eri_deriv_core(k).cpu().numpy()
+        data[f"eri_{n}_{n}_{n}_{n}_deriv{k}"] = np.ascontiguousarray(np.moveaxis(d, 0, -1))
+    return _write_datasets("eri_derivs", data)
+
+
+def compute_1e_deriv_disk(type_: str, max_deriv_order: int) -> str:
+    """Write one-electron derivative tensors to oei_derivs.(h5|npz): datasets
+    <type>_<n>_<n>_deriv<k>, shape (n, n, nderiv); first order in this build."""
+    return _oei_disk([type_], max_deriv_order)
+
+
+def oei_deriv_disk(max_deriv_order: int) -> str:
+    """Overlap, kinetic and potential derivative tensors to oei_derivs.(h5|npz)."""
+    return _oei_disk(list(_OEI_TYPES), max_deriv_order)
+
+
+def _oei_disk(types, max_deriv_order: int) -> str:
+    ks = [_oei_index(t) for t in types]
+    if max_deriv_order != 1:
+        raise NotImplementedError(f"one-electron derivative order {max_deriv_order} (this build: 1)")
+    eng = _engine()
+    n = eng.nbf
+    d = eng.oei_deriv(1)
+    data = {f"{_OEI_TYPES[k]}_{n}_{n}_deriv1": np.ascontiguousarray(np.moveaxis(d[k].cpu().numpy(), 0, -1))
+            for k in ks}
+    return _write_datasets("oei_derivs", data)
 
 
 # -- device-resident variants (additions) -------------------------------------------

@@ -36,9 +36,9 @@ class TEI:
         self.natom = self.engine.natom
         self.nbf = self.engine.nbf
         self.mode = mode
-        if mode == "disk":
-            raise NotImplementedError("HDF5 disk mode is not part of this build")
-        if mode not in ("core", "f12"):
+        # mode "disk" (tei.py:157-181): derivative slices are read from
+        # eri_derivs.(h5|npz) written by libint_interface.compute_2e_deriv_disk
+        if mode not in ("core", "f12", "disk"):
             raise ValueError(f"unknown mode {mode}")
         self.eri_derivatives = []
         if mode == "core" and max_deriv_order > 0:
@@ -63,6 +63,12 @@ class TEI:
             if order > len(self.eri_derivatives):
                 raise NotImplementedError(f"order {order} derivatives were not precomputed")
             return self.eri_derivatives[order - 1][get_deriv_vec_idx(dv)]
+        if self.mode == "disk":
+            from .libint_interface import read_dataset
+
+            n = self.nbf
+            data = read_dataset("eri_derivs", f"eri_{n}_{n}_{n}_{n}_deriv{order}")
+            return torch.from_numpy(np.ascontiguousarray(data[..., get_deriv_vec_idx(dv)])).to(self.engine.device)
         return self.engine.eri_deriv(dv)
 
     def eri_jvp(self, primals, tangents):

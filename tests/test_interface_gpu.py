@@ -87,3 +87,37 @@ def test_adjoint_autograd_against_finite_differences():
             e2.close()
         fd[nu] = (Es[0] - Es[1]) / (2 * h)
     assert np.abs(g.cpu().numpy() - fd).max() < 1e-6 * max(1.0, np.abs(fd).max())
+
+
+def test_disk_mode_roundtrip(tmp_path, monkeypatch):
+    """compute_2e_deriv_disk / oei_deriv_disk write the reference's datasets
+    (derivative index last; .npz where h5py is absent) and TEI(mode="disk") reads
+    the slices back."""
+    from quax_b200.integrals import libint_interface as li
+    from quax_b200.integrals.tei import TEI
+
+    monkeypatch.chdir(tmp_path)
+    mol = h2o_config1()
+    b = build_basis(mol, "sto-3g")
+    li.initialize_basis(b, 1e-14, charges=mol.Z)
+    try:
+        path = li.compute_2e_deriv_disk("eri", 0.0, 2)
+        n = b.nbf()
+        d1 = li.read_dataset("eri_derivs", f"eri_{n}_{n}_{n}_{n}_deriv1")
+        d2 = li.read_dataset("eri_derivs", f"eri_{n}_{n}_{n}_{n}_deriv2")
+        assert d1.shape == (n, n, n, n, 9) and d2.shape == (n, n, n, n, 45)
+        core = li.engine().eri_deriv_core(1).cpu().numpy()
+        assert np.abs(np.moveaxis(d1, -1, 0) - core).max() == 0.0
+        tei = TEI(b, mode="disk", engine=li.engine())
+        dv = np.zeros(9, dtype=int)
+        dv[3] = 1
+        dv[7] = 1
+        from quax_b200.utils import get_deriv_vec_idx
+
+        assert np.abs(tei.eri_deriv(None, dv).cpu().numpy() - d2[..., get_deriv_vec_idx(dv)]).max() == 0.0
+        li.oei_deriv_disk(1)
+        s1 = li.read_dataset("oei_derivs", f"overlap_{n}_{n}_deriv1")
+        assert s1.shape == (n, n, 9)
+        assert path.startswith("eri_derivs.")
+    finally:
+        li.finalize()
