@@ -266,6 +266,7 @@ struct qx_handle {
     int wpq[QX_NUM_CLASSES];        // warps per quartet, plain warp kernels
     int wpq_deriv[QX_NUM_CLASSES];  // warps per quartet, derivative warp kernels
     int shard_rank = 0, shard_n = 1;
+    int prim_stage = 0;  // split-mode VRR: primitive pairs staged per warp (2 x largest pair), 0 = off
     // J/K density screening: sqrt(K) and max |D| per pair record, threshold of the
     // call in progress (0 = off)
     double* d_kpair = nullptr;
@@ -455,7 +456,9 @@ static int run_class(qx_handle* h, int cls, int mode, const int2* d_q, long long
                 return fail(QX_E_NOMEM, "plain split-mode accumulators for class %d", cls);
             }
             QX_CUDA(cudaMemsetAsync(w.d_pacc, 0, sizeof(double) * w.nq * np, s));
-            g_pvrr[cls](a, w.d_dtasks, w.ndtask, qx_der_chunk(), w.d_pacc, (int)np, s);
+            EriArgs av = a;
+            av.prim_stage = h->prim_stage;
+            g_pvrr[cls](av, w.d_dtasks, w.ndtask, qx_der_chunk(), w.d_pacc, (int)np, s);
             wa.wpq = 1;
             wa.acc_in = w.d_pacc;
         }
@@ -592,6 +595,14 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
     std::vector<double> boys;
     boys_table_host(boys);
     const int np = (int)h->pairs.size();
+    {
+        // bulk-copy staging of the primitive pairs in the split-mode VRR kernels:
+        // room for one bra and one ket pair, up to 64 primitive pairs each (10 KB
+        // per warp); QX_NO_STAGE=1 reads them from global memory instead
+        int mx = 0;
+        for (const auto& pi : h->pairs) mx = std::max(mx, pi.nprim);
+        h->prim_stage = (mx <= 64 && !std::getenv("QX_NO_STAGE")) ? 2 * mx : 0;
+    }
 #define QX_ALLOC(ptr, bytes)                                                          \
     do {                                                                              \
         if (cudaMalloc((void**)&(ptr), (bytes)) != cudaSuccess) {                     \
@@ -1013,7 +1024,9 @@ static int run_deriv_class(qx_handle* h, int c, int mode, double* out, const dou
             const long long nt = w.slice_t[sl + 1] - w.slice_t[sl];
             if (h->deriv_eng[c] == ENG_WVRR) {
                 QX_CUDA(cudaMemsetAsync(w.d_dacc, 0, sizeof(double) * a.nq * nacc, cs));
-                g_wvrr[c](a, tk, nt, qx_der_chunk(), w.d_dacc, (int)nacc, cs);
+                EriArgs av = a;
+                av.prim_stage = h->prim_stage;
+                g_wvrr[c](av, tk, nt, qx_der_chunk(), w.d_dacc, (int)nacc, cs);
                 qx_launch_der_hrr(g_der_idx[c], a, mode, D, cj, ck, grad, slice, w.d_dacc, cs);
             } else {
                 qx_launch_der_split(g_der_idx[c], a, mode, D, cj, ck, grad, slice, tk, nt, w.d_dacc, cs);

@@ -33,6 +33,10 @@ struct EriArgs {
     const double* jk_kpair = nullptr;  // sqrt(Schwarz K) per pair record
     const double* jk_dmax = nullptr;   // max |D| per pair record
     double jk_thr = 0.0;
+    // split-mode VRR kernels: primitive-pair records a warp stages into shared
+    // memory with the bulk-copy (TMA) engine, bra and ket together; 0 = read them
+    // from global memory
+    int prim_stage = 0;
 };
 
 // True when density screening drops this quartet from J/K.

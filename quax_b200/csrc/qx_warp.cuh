@@ -102,6 +102,45 @@ struct GlobalSink {
     }
 };
 
+// Bulk copies global -> shared memory through the TMA unit (cp.async.bulk, no
+// tensor map, no multicast), completed on a shared-memory mbarrier.  The waits are
+// bounded: a copy that has not landed after `limit` polls makes the kernel report
+// an error word instead of spinning on.
+__device__ __forceinline__ unsigned qx_smem_u32(const void* p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void qx_mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(qx_smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void qx_mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(qx_smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// dst, src 16-byte aligned, bytes a multiple of 16
+__device__ __forceinline__ void qx_bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     qx_smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(qx_smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool qx_mbar_wait(unsigned long long* bar, unsigned phase, int limit) {
+    for (int it = 0; it < limit; ++it) {
+        unsigned done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(done)
+            : "r"(qx_smem_u32(bar)), "r"(phase)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
 // Chunked warp programs: the lane's VRR inputs are saved once per primitive
 // quartet (lane-strided, bank-conflict free) and every later chunk reloads them
 // with volatile loads, so the compiler cannot merge a chunk's recomputed
@@ -558,8 +597,33 @@ __global__ void __launch_bounds__(WARP_QPB * 32) k_gvrr(EriArgs a, const int2* _
     if (!DER && jk_screened(a, pq, P, Q)) return;  // J/K density screening (set only in J/K calls)
     double* qacc = acc + (size_t)task.x * (DER ? nacc : W::NITEM_PAD);
     const bool f32 = task.x >= a.nq64;  // warp-uniform: one task per warp
-    extern __shared__ double wv_sm[];
-    double* save = wv_sm + (size_t)(threadIdx.x >> 5) * W::SAVE;
+    // per-warp shared memory: [staged primitive pairs][mbarrier][chunk save area]
+    extern __shared__ __align__(16) double wv_sm[];
+    const int stage = a.prim_stage;
+    const size_t per_warp = (size_t)stage * (sizeof(PrimPair) / 8) + 2 + W::SAVE;
+    double* wbase = wv_sm + (size_t)(threadIdx.x >> 5) * per_warp;
+    PrimPair* sp = reinterpret_cast<PrimPair*>(wbase);
+    unsigned long long* bar = reinterpret_cast<unsigned long long*>(wbase + (size_t)stage * (sizeof(PrimPair) / 8));
+    double* save = wbase + (size_t)stage * (sizeof(PrimPair) / 8) + 2;
+    const PrimPair* bra = a.prims + P.prim_off;
+    const PrimPair* ket = a.prims + Q.prim_off;
+    if (stage) {
+        // the quartet's bra and ket primitive pairs, one bulk copy each
+        if (lane == 0) qx_mbar_init(bar, 1);
+        __syncwarp();
+        if (lane == 0) {
+            const unsigned bb = (unsigned)(P.nprim * sizeof(PrimPair)), kb = (unsigned)(Q.nprim * sizeof(PrimPair));
+            qx_mbar_expect_tx(bar, bb + kb);
+            qx_bulk_g2s(sp, bra, bb, bar);
+            qx_bulk_g2s(sp + P.nprim, ket, kb, bar);
+        }
+        if (!qx_mbar_wait(bar, 0, 1 << 22)) {
+            if (lane == 0 && a.err) atomicOr(a.err, 1);
+            return;
+        }
+        bra = sp;
+        ket = sp + P.nprim;
+    }
     const int nk = Q.nprim, ntot = P.nprim * nk;
     const int tend = min(ntot, task.y + chunk);
     for (int t0 = task.y; t0 < tend; t0 += 32) {
@@ -567,8 +631,8 @@ __global__ void __launch_bounds__(WARP_QPB * 32) k_gvrr(EriArgs a, const int2* _
         const bool act = t < tend;
         const int tt = act ? t : task.y;
         const int i = tt / nk, j = tt - i * nk;
-        const PrimPair p = a.prims[P.prim_off + i];
-        const PrimPair r = a.prims[Q.prim_off + j];
+        const PrimPair p = bra[i];
+        const PrimPair r = ket[j];
         PrimQ q;
         double Fp[W::S + 1];
         prim_setup<W::S>(p, r, a.boys, q, Fp);
@@ -601,7 +665,8 @@ template <class W, bool DER>
 void launch_gvrr(const EriArgs& a, const int2* tasks, long long ntask, int chunk, double* acc, int nacc,
                  cudaStream_t s) {
     const long long nb = (ntask + WARP_QPB - 1) / WARP_QPB;
-    const size_t smem = sizeof(double) * (size_t)W::SAVE * WARP_QPB;
+    const size_t per_warp = (size_t)a.prim_stage * (sizeof(PrimPair) / 8) + 2 + W::SAVE;
+    const size_t smem = sizeof(double) * per_warp * WARP_QPB;
     auto k = k_gvrr<W, DER>;
     if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (nb) k<<<(unsigned)nb, WARP_QPB * 32, smem, s>>>(a, tasks, ntask, chunk, acc, nacc);
