@@ -2,9 +2,9 @@
 
 The reference gets S, T, V and their derivative tensors from Libint
 (quax/integrals/libint_interface.cc:101-155, 231-483, 2403-2581; quax/integrals/oei.py).
-They are O(n^2) work, outside the two-electron kernels; the RHF driver of this
-package needs them for the energy and the analytic gradient, so they are computed
-here in FP64 with the McMurchie-Davidson scheme (Hermite expansion coefficients
+The library computes them on the GPU (qx_oei, qx_oei_deriv_core); this host
+version is the independent check the tests compare the GPU kernel with, and the
+nuclear-repulsion term of the RHF driver.  FP64, McMurchie-Davidson scheme (Hermite expansion coefficients
 E^{ij}_t and Hermite Coulomb integrals R_tuv; McMurchie & Davidson, J. Comput.
 Phys. 26, 218 (1978)).  Derivatives use d/dA_x g_a = 2 alpha g_{a+1x} - a_x g_{a-1x}
 on both centres; the derivative with respect to a nucleus in V follows from
