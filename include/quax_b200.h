@@ -218,7 +218,8 @@ int qx_autotune(qx_handle *h, int what, void *stream);
  * 1 warp, 2 cooperative, 4 warp VRR into global accumulators + warp HRR),
  * cfg[1] its parameter (log2 lanes per quartet, or warps per quartet), cfg[2]
  * derivative engine (1 warp, 2 cooperative, 3 warp VRR into
- * global accumulators + cooperative HRR), cfg[3] its warps per quartet. */
+ * global accumulators + cooperative HRR, 5 warp VRR into global accumulators +
+ * warp HRR), cfg[3] its warps per quartet. */
 int qx_engine_config(const qx_handle *h, int cls, int *cfg);
 
 /* Size of the fixed device array qx_compute_2e_int_noalloc works in. */

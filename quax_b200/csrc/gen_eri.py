@@ -1064,6 +1064,11 @@ def gen_warp_code(cid, la, lb, lc, ld, deriv, p, want_warp=True, want_wvrr=False
         L.append(f"void qx_launch_{kind}_{tag}(const qx::EriArgs& a, const int2* tasks, long long ntask, int chunk, "
                  f"double* acc, int nacc, cudaStream_t s) "
                  f"{{ qx::launch_gvrr<Warp_{tag}, {'true' if deriv else 'false'}>(a, tasks, ntask, chunk, acc, nacc, s); }}")
+    if want_wvrr and want_warp and deriv == 1:
+        # derivative split with the warp HRR: items kept in item order
+        L.append(f"void qx_launch_dsplit_{tag}(const qx::EriArgs& a, const int2* tasks, long long ntask, int chunk, "
+                 f"double* acc, int nacc, cudaStream_t s) "
+                 f"{{ qx::launch_gvrr<Warp_{tag}, true, true>(a, tasks, ntask, chunk, acc, nacc, s); }}")
     return "\n".join(L)
 
 
@@ -1150,6 +1155,9 @@ def main():
         f.write("#define QX_FOR_EACH_WARP_PLAIN(X) " + " ".join(f"X({i:02d})" for i, x in enumerate(wp) if x) + "\n")
         f.write("#define QX_FOR_EACH_WARP_DERIV(X) " + " ".join(f"X({i:02d})" for i, x in enumerate(wd) if x) + "\n")
         f.write("#define QX_CLASS_WVRR {" + ", ".join("1" if x else "0" for x in wv) + "}\n")
+        ds = [okd_ and okv_ for okd_, okv_ in zip(wd, wv)]
+        f.write("#define QX_CLASS_DSPLIT {" + ", ".join("1" if x else "0" for x in ds) + "}\n")
+        f.write("#define QX_FOR_EACH_DSPLIT(X) " + " ".join(f"X({i:02d})" for i, x in enumerate(ds) if x) + "\n")
         f.write("#define QX_CLASS_PVRR {" + ", ".join("1" if x else "0" for x in wq) + "}\n")
         f.write("#define QX_FOR_EACH_PVRR(X) " + " ".join(f"X({i:02d})" for i, x in enumerate(wq) if x) + "\n")
         f.write("#define QX_FOR_EACH_WVRR(X) " + " ".join(f"X({i:02d})" for i, x in enumerate(wv) if x) + "\n")

@@ -95,11 +95,13 @@ static const int g_has_warp_plain[QX_NUM_CLASSES] = QX_CLASS_WARP_PLAIN;
 static const int g_has_warp_deriv[QX_NUM_CLASSES] = QX_CLASS_WARP_DERIV;
 static const int g_has_wvrr[QX_NUM_CLASSES] = QX_CLASS_WVRR;
 static const int g_has_pvrr[QX_NUM_CLASSES] = QX_CLASS_PVRR;
+static const int g_has_dsplit[QX_NUM_CLASSES] = QX_CLASS_DSPLIT;
 static WarpLaunch g_warp_plain[QX_NUM_CLASSES];
 static WarpLaunch g_warp_deriv[QX_NUM_CLASSES];
 static WarpLaunch g_warp_deriv2[QX_NUM_CLASSES];  // second derivatives (classes with l <= 1)
 static WvrrLaunch g_wvrr[QX_NUM_CLASSES];          // derivative VRR into global accumulators
 static WvrrLaunch g_pvrr[QX_NUM_CLASSES];          // plain VRR into global accumulators
+static WvrrLaunch g_dsplit[QX_NUM_CLASSES];        // derivative VRR into item-order accumulators
 #define QX_DECL_WP(id) void qx_launch_warp_p##id(const qx::WarpArgs&, int, cudaStream_t);
 QX_FOR_EACH_WARP_PLAIN(QX_DECL_WP)
 #define QX_DECL_WD(id) void qx_launch_warp_d##id(const qx::WarpArgs&, int, cudaStream_t);
@@ -112,13 +114,18 @@ QX_FOR_EACH_WVRR(QX_DECL_WV)
 #define QX_DECL_PV(id) \
     void qx_launch_pvrr_p##id(const qx::EriArgs&, const int2*, long long, int, double*, int, cudaStream_t);
 QX_FOR_EACH_PVRR(QX_DECL_PV)
+#define QX_DECL_DS(id) \
+    void qx_launch_dsplit_d##id(const qx::EriArgs&, const int2*, long long, int, double*, int, cudaStream_t);
+QX_FOR_EACH_DSPLIT(QX_DECL_DS)
 // Engines per class.  Plain ERI: straight-line per-thread kernels (small classes),
 // warp-per-quartet kernels (lanes = primitive quartets), or the cooperative engine
 // (classes whose VRR does not fit a lane's registers).  Derivatives: warp kernels
 // where they fit, else the cooperative derivative engine.
 // ENG_WVRR (derivatives): warp-program VRR into global accumulators + the
 // cooperative HRR; ENG_WSPLIT (plain): the same VRR split + the warp HRR.
-enum { ENG_SL = 0, ENG_WARP = 1, ENG_COOP = 2, ENG_WVRR = 3, ENG_WSPLIT = 4 };
+// ENG_DSPLIT (derivatives): the split VRR into item-order accumulators + the warp
+// kernel's own HRR and epilogue.
+enum { ENG_SL = 0, ENG_WARP = 1, ENG_COOP = 2, ENG_WVRR = 3, ENG_WSPLIT = 4, ENG_DSPLIT = 5 };
 int qx_der_index(int cls);
 void qx_launch_der_split(int der_idx, const qx::EriArgs& a, int mode, const double* D, double cj, double ck,
                          double* grad, int slice, const int2* tasks, long long ntask, double* scratch, cudaStream_t s);
@@ -141,6 +148,7 @@ static bool init_class_tables() {
         g_warp_deriv2[c] = nullptr;
         g_wvrr[c] = nullptr;
         g_pvrr[c] = nullptr;
+        g_dsplit[c] = nullptr;
     }
 #define QX_SET_WP(id) g_warp_plain[1##id - 100] = &qx_launch_warp_p##id;
     QX_FOR_EACH_WARP_PLAIN(QX_SET_WP)
@@ -152,6 +160,8 @@ static bool init_class_tables() {
     QX_FOR_EACH_WVRR(QX_SET_WV)
 #define QX_SET_PV(id) g_pvrr[1##id - 100] = &qx_launch_pvrr_p##id;
     QX_FOR_EACH_PVRR(QX_SET_PV)
+#define QX_SET_DS(id) g_dsplit[1##id - 100] = &qx_launch_dsplit_d##id;
+    QX_FOR_EACH_DSPLIT(QX_SET_DS)
 #define QX_SL_ENTRY(id, a, b, c, d)                            \
     g_eri_launch[id] = &qx_launch_eri_##id;                    \
     g_class_scratch[id] = qx::scratch_per_quartet<a, b, c, d>();
@@ -327,7 +337,8 @@ static int ensure_split_tasks(qx_handle* h, int c, bool need_dacc = false, const
         if (sync) QX_CUDA(cudaDeviceSynchronize());
     }
     if (need_dacc && !w.d_dacc &&
-        cudaMalloc((void**)&w.d_dacc, sizeof(double) * std::min(w.nq, cap_q) * nacc) != cudaSuccess) {
+        cudaMalloc((void**)&w.d_dacc, sizeof(double) * std::min(w.nq, cap_q) * ((nacc + 15) / 16 * 16)) !=
+            cudaSuccess) {
         cudaGetLastError();
         w.d_dacc = nullptr;
         return fail(QX_E_NOMEM, "split-mode derivative accumulators for class %d", c);
@@ -364,13 +375,16 @@ static void choose_engines(qx_handle* h) {
             if (!std::strcmp(pe, "coop") && g_class_coop[c]) p = ENG_COOP;
             if (!std::strcmp(pe, "wsplit") && g_has_pvrr[c]) p = ENG_WSPLIT;
         }
-        // the global-accumulator VRR wins for the classes with L >= 6 (measured);
-        // the autotuner settles the rest per molecule
+        // split VRR with the warp HRR where the class has it, else the split VRR with
+        // the cooperative HRR for L >= 6 (measured on the 10-atom workload); the
+        // autotuner settles each class per molecule
         const int L = g_class_l[c][0] + g_class_l[c][1] + g_class_l[c][2] + g_class_l[c][3];
-        int d = (g_has_wvrr[c] && (L >= 6 || !g_has_warp_deriv[c])) ? ENG_WVRR
+        int d = g_has_dsplit[c] ? ENG_DSPLIT
+                : (g_has_wvrr[c] && (L >= 6 || !g_has_warp_deriv[c])) ? ENG_WVRR
                 : (g_has_warp_deriv[c] ? ENG_WARP : ENG_COOP);
         if (de && !std::strcmp(de, "coop")) d = ENG_COOP;
         if (de && !std::strcmp(de, "wvrr") && g_has_wvrr[c]) d = ENG_WVRR;
+        if (de && !std::strcmp(de, "dsplit") && g_has_dsplit[c]) d = ENG_DSPLIT;
         h->plain_eng[c] = p;
         h->deriv_eng[c] = d;
     }
@@ -1028,6 +1042,22 @@ static int run_deriv_class(qx_handle* h, int c, int mode, double* out, const dou
                 av.prim_stage = h->prim_stage;
                 g_wvrr[c](av, tk, nt, qx_der_chunk(), w.d_dacc, (int)nacc, cs);
                 qx_launch_der_hrr(g_der_idx[c], a, mode, D, cj, ck, grad, slice, w.d_dacc, cs);
+            } else if (h->deriv_eng[c] == ENG_DSPLIT) {
+                const long long npad = (nacc + 15) / 16 * 16;  // the warp program's NITEM_PAD
+                QX_CUDA(cudaMemsetAsync(w.d_dacc, 0, sizeof(double) * a.nq * npad, cs));
+                EriArgs av = a;
+                av.prim_stage = h->prim_stage;
+                g_dsplit[c](av, tk, nt, qx_der_chunk(), w.d_dacc, (int)npad, cs);
+                WarpArgs wa;
+                wa.e = a;
+                wa.wpq = 1;
+                wa.D = D;
+                wa.cj = cj;
+                wa.ck = ck;
+                wa.grad = grad;
+                wa.slice = slice;
+                wa.acc_in = w.d_dacc;
+                g_warp_deriv[c](wa, mode, cs);
             } else {
                 qx_launch_der_split(g_der_idx[c], a, mode, D, cj, ck, grad, slice, tk, nt, w.d_dacc, cs);
             }
@@ -1408,6 +1438,7 @@ extern "C" int qx_autotune(qx_handle* h, int what, void* stream) {
                 cand.push_back({ENG_WARP, 4});
             }
             if (g_has_wvrr[c]) cand.push_back({ENG_WVRR, 0});
+            if (g_has_dsplit[c]) cand.push_back({ENG_DSPLIT, 0});
             if (g_der_idx[c] >= 0) cand.push_back({ENG_COOP, 0});
             float best = 1e30f;
             TuneCfg bc{h->deriv_eng[c], h->wpq_deriv[c]};

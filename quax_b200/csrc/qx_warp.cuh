@@ -583,7 +583,7 @@ typedef void (*WarpLaunch)(const WarpArgs&, int mode, cudaStream_t);
 // cooperative engine's accumulator layout (nacc per quartet); plain programs keep
 // the item order (NITEM_PAD per quartet).  Task quartet indices are relative to
 // a.quartets; acc must be zeroed before the launch.
-template <class W, bool DER>
+template <class W, bool DER, bool ITEMS = false>
 __global__ void __launch_bounds__(WARP_QPB * 32) k_gvrr(EriArgs a, const int2* __restrict__ tasks, long long ntask,
                                                          int chunk, double* __restrict__ acc, int nacc) {
     const unsigned lane = threadIdx.x & 31;
@@ -595,7 +595,9 @@ __global__ void __launch_bounds__(WARP_QPB * 32) k_gvrr(EriArgs a, const int2* _
     const PairInfo Q = a.pairs[pq.y];
     if (DER && P.atom1 == P.atom2 && P.atom1 == Q.atom1 && P.atom1 == Q.atom2) return;  // reference skips these
     if (!DER && jk_screened(a, pq, P, Q)) return;  // J/K density screening (set only in J/K calls)
-    double* qacc = acc + (size_t)task.x * (DER ? nacc : W::NITEM_PAD);
+    // ITEMS: derivative items kept in item order (NITEM_PAD per quartet) for the
+    // warp kernel's own HRR instead of the cooperative layout
+    double* qacc = acc + (size_t)task.x * ((DER && !ITEMS) ? nacc : W::NITEM_PAD);
     const bool f32 = task.x >= a.nq64;  // warp-uniform: one task per warp
     // per-warp shared memory: [staged primitive pairs][mbarrier][chunk save area]
     extern __shared__ __align__(16) double wv_sm[];
@@ -647,12 +649,12 @@ __global__ void __launch_bounds__(WARP_QPB * 32) k_gvrr(EriArgs a, const int2* _
             for (int m = 0; m <= W::S; ++m) Ff[m] = (float)Fp[m];
             const PrimQT<float> qf = qx_to_float(q);
             float* sf = reinterpret_cast<float*>(save);
-            if constexpr (DER)
+            if constexpr (DER && !ITEMS)
                 W::vrr(Ff, qf, wa, wb, wc, GlobalSink{qacc, W::vmap()}, lane, sf);
             else
                 W::vrr(Ff, qf, wa, wb, wc, IdentSink{qacc}, lane, sf);
         } else {
-            if constexpr (DER)
+            if constexpr (DER && !ITEMS)
                 W::vrr(Fp, q, wa, wb, wc, GlobalSink{qacc, W::vmap()}, lane, save);
             else
                 W::vrr(Fp, q, wa, wb, wc, IdentSink{qacc}, lane, save);
@@ -661,13 +663,13 @@ __global__ void __launch_bounds__(WARP_QPB * 32) k_gvrr(EriArgs a, const int2* _
     }
 }
 
-template <class W, bool DER>
+template <class W, bool DER, bool ITEMS = false>
 void launch_gvrr(const EriArgs& a, const int2* tasks, long long ntask, int chunk, double* acc, int nacc,
                  cudaStream_t s) {
     const long long nb = (ntask + WARP_QPB - 1) / WARP_QPB;
     const size_t per_warp = (size_t)a.prim_stage * (sizeof(PrimPair) / 8) + 2 + W::SAVE;
     const size_t smem = sizeof(double) * per_warp * WARP_QPB;
-    auto k = k_gvrr<W, DER>;
+    auto k = k_gvrr<W, DER, ITEMS>;
     if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (nb) k<<<(unsigned)nb, WARP_QPB * 32, smem, s>>>(a, tasks, ntask, chunk, acc, nacc);
 }

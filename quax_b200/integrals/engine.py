@@ -188,7 +188,7 @@ class EriEngine:
             )
         return out
 
-    ENGINE_NAMES = ("sl", "warp", "coop", "wvrr", "wsplit")
+    ENGINE_NAMES = ("sl", "warp", "coop", "wvrr", "wsplit", "dsplit")
 
     def autotune(self, plain: bool = True, deriv: bool = True, stream=None) -> None:
         """Time every engine configuration per class on this molecule and keep the fastest."""
