@@ -24,6 +24,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "quax_b200.h"
@@ -693,14 +694,41 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
                 kept.push_back(pair_index(s1, s2));
                 kk.push_back(h->K[(size_t)s1 * nshell + s2]);
             }
+    // pair-pair enumeration, split over host threads in contiguous ranges of i of
+    // equal work (~i^2 / 2) and concatenated in order, so the lists are the same
+    // as a serial pass
     std::vector<std::vector<int2>> lists(QX_NUM_CLASSES);
-    for (size_t i = 0; i < kept.size(); ++i)
-        for (size_t j = 0; j <= i; ++j) {
-            if (kk[i] * kk[j] < thr2) continue;
-            int pb = kept[i], pk = kept[j];
-            if (h->pcls[pb] < h->pcls[pk]) std::swap(pb, pk);
-            lists[quartet_class(h->pcls[pb], h->pcls[pk])].push_back(make_int2(pb, pk));
+    {
+        const size_t nk = kept.size();
+        const int nt = (int)std::max<size_t>(1, std::min<size_t>(std::thread::hardware_concurrency(),
+                                                                  std::max<size_t>(1, nk / 256)));
+        std::vector<size_t> cut_i(nt + 1, nk);
+        cut_i[0] = 0;
+        for (int t = 1; t < nt; ++t) cut_i[t] = (size_t)(nk * std::sqrt((double)t / nt));
+        std::vector<std::vector<std::vector<int2>>> part(nt, std::vector<std::vector<int2>>(QX_NUM_CLASSES));
+        auto work = [&](int t) {
+            for (size_t i = cut_i[t]; i < cut_i[t + 1]; ++i)
+                for (size_t j = 0; j <= i; ++j) {
+                    if (kk[i] * kk[j] < thr2) continue;
+                    int pb = kept[i], pk = kept[j];
+                    if (h->pcls[pb] < h->pcls[pk]) std::swap(pb, pk);
+                    part[t][quartet_class(h->pcls[pb], h->pcls[pk])].push_back(make_int2(pb, pk));
+                }
+        };
+        std::vector<std::thread> pool;
+        for (int t = 1; t < nt; ++t) pool.emplace_back(work, t);
+        work(0);
+        for (auto& th : pool) th.join();
+        for (int c = 0; c < QX_NUM_CLASSES; ++c) {
+            size_t tot = 0;
+            for (int t = 0; t < nt; ++t) tot += part[t][c].size();
+            lists[c].reserve(tot);
+            for (int t = 0; t < nt; ++t) {
+                lists[c].insert(lists[c].end(), part[t][c].begin(), part[t][c].end());
+                std::vector<int2>().swap(part[t][c]);
+            }
         }
+    }
     long long base = 0;
     for (int c = 0; c < QX_NUM_CLASSES; ++c) {
         auto& L = lists[c];
