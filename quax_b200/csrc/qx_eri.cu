@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <chrono>
 #include <functional>
+#include <memory>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -296,6 +297,15 @@ struct qx_handle {
 // most QX_SPLIT_ACC_BYTES of derivative accumulators; each slice runs as its own
 // VRR + HRR pair.  `list` is the class's current view when the caller has it on
 // the host (set-up), else it is copied back from the device.
+// Runs f(0..nt-1) on nt host threads (f(0) on the caller's).
+template <class F>
+static void host_parallel(int nt, F&& f) {
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t) pool.emplace_back([&f, t] { f(t); });
+    f(0);
+    for (auto& th : pool) th.join();
+}
+
 static int ensure_split_tasks(qx_handle* h, int c, bool need_dacc = false, const int2* list = nullptr,
                               bool sync = true) {
     ClassWork& w = h->work[c];
@@ -309,29 +319,48 @@ static int ensure_split_tasks(qx_handle* h, int c, bool need_dacc = false, const
             QX_CUDA(cudaMemcpy(L.data(), w.d_q, sizeof(int2) * w.nq, cudaMemcpyDeviceToHost));
             list = L.data();
         }
-        std::vector<int2> tasks;
-        w.slice_q.assign(1, 0);
-        w.slice_t.assign(1, 0);
+        // tasks (slice-relative quartet, first primitive quartet), ch primitive
+        // quartets each; slices of cap_q quartets.  Built over host threads: each
+        // counts the tasks of a contiguous quartet range, then writes them after an
+        // exclusive scan, recording the task offset of the slice starts in its range.
         const int ch = qx_der_chunk();
-        long long q0 = 0;
-        for (long long qi = 0; qi < w.nq; ++qi) {
-            if (qi - q0 == cap_q) {
-                q0 = qi;
-                w.slice_q.push_back(qi);
-                w.slice_t.push_back((long long)tasks.size());
-            }
+        const long long nslice = (w.nq + cap_q - 1) / cap_q;
+        const int nt = (int)std::max(1LL, std::min<long long>(std::max(1u, std::thread::hardware_concurrency()),
+                                                              w.nq / 65536));
+        std::vector<long long> tcount(nt + 1, 0);
+        auto q_lo = [&](int t) { return w.nq * t / nt; };
+        auto ntask = [&](long long qi) {
             const int np_q = h->pairs[list[qi].x].nprim * h->pairs[list[qi].y].nprim;
-            for (int t0 = 0; t0 < np_q; t0 += ch) tasks.push_back(make_int2((int)(qi - q0), t0));
-        }
-        w.slice_q.push_back(w.nq);
-        w.slice_t.push_back((long long)tasks.size());
-        if (cudaMalloc((void**)&w.d_dtasks, sizeof(int2) * tasks.size()) != cudaSuccess) {
+            return (long long)((np_q + ch - 1) / ch);
+        };
+        host_parallel(nt, [&](int t) {
+            long long n = 0;
+            for (long long qi = q_lo(t); qi < q_lo(t + 1); ++qi) n += ntask(qi);
+            tcount[t + 1] = n;
+        });
+        for (int t = 0; t < nt; ++t) tcount[t + 1] += tcount[t];
+        const long long ntot = tcount[nt];
+        std::unique_ptr<int2[]> tasks(new int2[(size_t)std::max(1LL, ntot)]);
+        w.slice_q.assign((size_t)nslice + 1, 0);
+        w.slice_t.assign((size_t)nslice + 1, 0);
+        for (long long k = 0; k <= nslice; ++k) w.slice_q[k] = std::min(w.nq, k * cap_q);
+        w.slice_t[nslice] = ntot;
+        host_parallel(nt, [&](int t) {
+            long long pos = tcount[t];
+            for (long long qi = q_lo(t); qi < q_lo(t + 1); ++qi) {
+                if (qi % cap_q == 0) w.slice_t[qi / cap_q] = pos;
+                const int rel = (int)(qi % cap_q);
+                const int np_q = h->pairs[list[qi].x].nprim * h->pairs[list[qi].y].nprim;
+                for (int t0 = 0; t0 < np_q; t0 += ch) tasks[pos++] = make_int2(rel, t0);
+            }
+        });
+        if (cudaMalloc((void**)&w.d_dtasks, sizeof(int2) * std::max(1LL, ntot)) != cudaSuccess) {
             cudaGetLastError();
             w.d_dtasks = nullptr;
             return fail(QX_E_NOMEM, "split-mode tasks for class %d", c);
         }
-        w.ndtask = (long long)tasks.size();
-        QX_CUDA(cudaMemcpy(w.d_dtasks, tasks.data(), sizeof(int2) * tasks.size(), cudaMemcpyHostToDevice));
+        w.ndtask = ntot;
+        QX_CUDA(cudaMemcpy(w.d_dtasks, tasks.get(), sizeof(int2) * ntot, cudaMemcpyHostToDevice));
         // a pageable host-to-device copy may still be in flight when cudaMemcpy
         // returns, and the kernels that read the tasks run on non-blocking streams
         // (set-up synchronises once at its end instead)
@@ -694,74 +723,81 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
                 kept.push_back(pair_index(s1, s2));
                 kk.push_back(h->K[(size_t)s1 * nshell + s2]);
             }
-    // pair-pair enumeration, split over host threads in contiguous ranges of i of
-    // equal work (~i^2 / 2) and concatenated in order, so the lists are the same
-    // as a serial pass
-    std::vector<std::vector<int2>> lists(QX_NUM_CLASSES);
-    {
-        const size_t nk = kept.size();
-        const int nt = (int)std::max<size_t>(1, std::min<size_t>(std::thread::hardware_concurrency(),
-                                                                  std::max<size_t>(1, nk / 256)));
-        std::vector<size_t> cut_i(nt + 1, nk);
-        cut_i[0] = 0;
-        for (int t = 1; t < nt; ++t) cut_i[t] = (size_t)(nk * std::sqrt((double)t / nt));
-        std::vector<std::vector<std::vector<int2>>> part(nt, std::vector<std::vector<int2>>(QX_NUM_CLASSES));
-        auto work = [&](int t) {
-            for (size_t i = cut_i[t]; i < cut_i[t + 1]; ++i)
-                for (size_t j = 0; j <= i; ++j) {
-                    if (kk[i] * kk[j] < thr2) continue;
-                    int pb = kept[i], pk = kept[j];
-                    if (h->pcls[pb] < h->pcls[pk]) std::swap(pb, pk);
-                    part[t][quartet_class(h->pcls[pb], h->pcls[pk])].push_back(make_int2(pb, pk));
-                }
-        };
-        std::vector<std::thread> pool;
-        for (int t = 1; t < nt; ++t) pool.emplace_back(work, t);
-        work(0);
-        for (auto& th : pool) th.join();
-        for (int c = 0; c < QX_NUM_CLASSES; ++c) {
-            size_t tot = 0;
-            for (int t = 0; t < nt; ++t) tot += part[t][c].size();
-            lists[c].reserve(tot);
-            for (int t = 0; t < nt; ++t) {
-                lists[c].insert(lists[c].end(), part[t][c].begin(), part[t][c].end());
-                std::vector<int2>().swap(part[t][c]);
+    // Pair-pair enumeration and the per-class counting sort by (bra nprim, ket
+    // nprim), largest first (equal trip counts within a warp, the cheap quartets in
+    // the tail of a launch), as a two-pass stable counting sort over host threads:
+    // thread t takes a contiguous range of i of about equal work (~i^2 / 2), counts
+    // its quartets per (class, key), and after an exclusive scan in (key, thread)
+    // order writes them straight to their sorted positions -- the same lists as a
+    // serial enumeration followed by a stable sort.
+    constexpr int NKEY = 64 * 64;
+    const size_t nk = kept.size();
+    const int nt = (int)std::max<size_t>(
+        1, std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), std::max<size_t>(1, nk / 256)));
+    std::vector<size_t> cut_i(nt + 1, nk);
+    cut_i[0] = 0;
+    for (int t = 1; t < nt; ++t) cut_i[t] = (size_t)(nk * std::sqrt((double)t / nt));
+    auto key = [&](int pb, int pk) {
+        return NKEY - 1 - std::min((h->pairs[pb].nprim - 1) * 64 + (h->pairs[pk].nprim - 1), NKEY - 1);
+    };
+    auto visit = [&](int t, auto&& fn) {
+        for (size_t i = cut_i[t]; i < cut_i[t + 1]; ++i)
+            for (size_t j = 0; j <= i; ++j) {
+                if (kk[i] * kk[j] < thr2) continue;
+                int pb = kept[i], pk = kept[j];
+                if (h->pcls[pb] < h->pcls[pk]) std::swap(pb, pk);
+                fn(quartet_class(h->pcls[pb], h->pcls[pk]), key(pb, pk), pb, pk);
             }
-        }
+    };
+    std::vector<long long> cnt((size_t)nt * QX_NUM_CLASSES * NKEY, 0);
+    std::vector<long long> tprims((size_t)nt * QX_NUM_CLASSES, 0);
+    host_parallel(nt, [&](int t) {
+        long long* C = cnt.data() + (size_t)t * QX_NUM_CLASSES * NKEY;
+        long long* P = tprims.data() + (size_t)t * QX_NUM_CLASSES;
+        visit(t, [&](int c, int k, int pb, int pk) {
+            C[(size_t)c * NKEY + k]++;
+            P[c] += (long long)h->pairs[pb].nprim * h->pairs[pk].nprim;
+        });
+    });
+    std::vector<long long> nq_c(QX_NUM_CLASSES, 0), prims_c(QX_NUM_CLASSES, 0);
+    for (int c = 0; c < QX_NUM_CLASSES; ++c) {
+        long long run = 0;
+        for (int k = 0; k < NKEY; ++k)
+            for (int t = 0; t < nt; ++t) {
+                long long& x = cnt[((size_t)t * QX_NUM_CLASSES + c) * NKEY + k];
+                const long long v = x;
+                x = run;
+                run += v;
+            }
+        nq_c[c] = run;
+        for (int t = 0; t < nt; ++t) prims_c[c] += tprims[(size_t)t * QX_NUM_CLASSES + c];
     }
+    std::vector<std::unique_ptr<int2[]>> sorted(QX_NUM_CLASSES);
+    for (int c = 0; c < QX_NUM_CLASSES; ++c)
+        if (nq_c[c]) sorted[c].reset(new int2[(size_t)nq_c[c]]);
+    host_parallel(nt, [&](int t) {
+        long long* C = cnt.data() + (size_t)t * QX_NUM_CLASSES * NKEY;
+        visit(t, [&](int c, int k, int pb, int pk) { sorted[c][C[(size_t)c * NKEY + k]++] = make_int2(pb, pk); });
+    });
+    std::vector<long long>().swap(cnt);
+    trace.mark("quartet enumeration, sort");
     long long base = 0;
     for (int c = 0; c < QX_NUM_CLASSES; ++c) {
-        auto& L = lists[c];
-        // counting sort by (bra nprim, ket nprim), largest first: equal trip counts
-        // within a warp and the cheap quartets in the tail of the launch
-        const int NK = 64 * 64;
-        std::vector<long long> cnt(NK + 1, 0);
-        auto key = [&](const int2& q) {
-            return NK - 1 - std::min((h->pairs[q.x].nprim - 1) * 64 + (h->pairs[q.y].nprim - 1), NK - 1);
-        };
-        long long prims = 0;
-        for (auto& q : L) {
-            cnt[key(q) + 1]++;
-            prims += (long long)h->pairs[q.x].nprim * h->pairs[q.y].nprim;
-        }
-        for (int k = 0; k < NK; ++k) cnt[k + 1] += cnt[k];
-        std::vector<int2> sorted(L.size());
-        for (auto& q : L) sorted[cnt[key(q)]++] = q;
         ClassWork& w = h->work[c];
-        w.nq = (long long)sorted.size();
-        w.prims = prims;
-        w.log2g = h->plain_eng[c] == ENG_SL ? choose_log2g(w.nq, prims) : 0;
-        h->wpq[c] = h->wpq_deriv[c] = choose_wpq(w.nq, prims);
+        w.nq = nq_c[c];
+        w.prims = prims_c[c];
+        w.log2g = h->plain_eng[c] == ENG_SL ? choose_log2g(w.nq, w.prims) : 0;
+        h->wpq[c] = h->wpq_deriv[c] = choose_wpq(w.nq, w.prims);
         w.unique_base = base;
         base += w.nq * g_class_nout[c];
         h->nunique += w.nq;
         if (w.nq) {
             QX_ALLOC(w.d_q, sizeof(int2) * w.nq);
-            cudaMemcpy(w.d_q, sorted.data(), sizeof(int2) * w.nq, cudaMemcpyHostToDevice);
+            cudaMemcpy(w.d_q, sorted[c].get(), sizeof(int2) * w.nq, cudaMemcpyHostToDevice);
             w.d_q_full = w.d_q;
             w.nq_full = w.nq;
             if (h->plain_eng[c] == ENG_WSPLIT) {
-                int rc = ensure_split_tasks(h, c, false, sorted.data(), false);
+                int rc = ensure_split_tasks(h, c, false, sorted[c].get(), false);
                 if (rc) {
                     free_handle(h);
                     return rc;
@@ -769,10 +805,11 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
             }
             if (g_class_scratch[c] && h->plain_eng[c] == ENG_SL)
                 QX_ALLOC(w.scratch, sizeof(double) * g_class_scratch[c] * launch_threads(w.nq, w.log2g));
+            sorted[c].reset();
         }
     }
     h->unique_size = base;
-    trace.mark("quartet lists, split tasks");
+    trace.mark("list uploads, split tasks");
     for (int c = 0; c < QX_NUM_CLASSES; ++c) h->order[c] = c;
     std::sort(h->order, h->order + QX_NUM_CLASSES,
               [&](int x, int y) { return h->work[x].prims * g_class_nout[x] > h->work[y].prims * g_class_nout[y]; });
