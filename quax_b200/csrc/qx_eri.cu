@@ -388,7 +388,7 @@ static int choose_wpq(long long nq, long long prims) {
 }
 
 // Default engine choice, overridable with QX_PLAIN_ENGINE=sl|warp|coop|wsplit and
-// QX_DERIV_ENGINE=coop|wvrr (for measuring alternatives); an override that a class
+// QX_DERIV_ENGINE=coop|wvrr|dsplit (for measuring alternatives); an override that a class
 // cannot honour falls back to the default.
 static void choose_engines(qx_handle* h) {
     const char* pe = std::getenv("QX_PLAIN_ENGINE");
