@@ -40,8 +40,8 @@ extern "C" {
 #define QX_E_NOMEM (-4)       /* device allocation failed */
 #define QX_E_DEVICE (-5)      /* a kernel reported an error through the error word */
 
-/* Highest angular momentum per shell compiled into this build. */
-#define QX_MAX_L 2
+/* Highest angular momentum per shell compiled into this build (f shells). */
+#define QX_MAX_L 3
 
 typedef struct qx_handle qx_handle;
 
@@ -98,18 +98,19 @@ int qx_compute_2e_int(qx_handle *h, double *out, int out_on_device, void *stream
 int qx_eri_unique(qx_handle *h, double *out_dev, void *stream);
 
 /* Replaces eri_deriv_core(order) (libint_interface.cc:2582-2779): the full
- * derivative tensor of order 1 or 2.  Order 1: 3N*n^4 doubles, layout
- * (3N, n, n, n, n), nuclear index 3*atom + xyz.  Order 2: M(M+1)/2 * n^4 doubles
- * (M = 3N), one slice per nuclear pair nu1 <= nu2 in the reference's
- * combinations-with-repetition order (utils.h:158-172, rank = nu1*M -
- * nu1(nu1-1)/2 + nu2 - nu1).  Quartets whose four shells sit on one atom are
- * skipped (zero), as in the reference.  Order 2 needs s and p shells only
- * (QX_E_UNSUPPORTED otherwise). */
+ * derivative tensor of order 1 to 4.  Order 1: 3N*n^4 doubles, layout
+ * (3N, n, n, n, n), nuclear index 3*atom + xyz.  Order k: C(M+k-1, k) * n^4
+ * doubles (M = 3N), one slice per sorted nuclear multi-index nu1 <= ... <= nuk in
+ * the reference's combinations-with-repetition order (utils.h:158-172; order 2:
+ * rank = nu1*M - nu1(nu1-1)/2 + nu2 - nu1), each the sum over the shells on the
+ * atoms of nu (the reference's cartesian product of shell choices,
+ * libint_interface.cc:1200-1226).  Quartets whose four shells sit on one atom are
+ * skipped (zero), as in the reference. */
 int qx_eri_deriv_core(qx_handle *h, int order, double *out, int out_on_device, void *stream);
 
 /* Replaces compute_2e_deriv("eri", 0., deriv_vec) (libint_interface.cc:1097-1335):
  * one n^4 derivative slice selected by deriv_vec[3*natom] (non-negative counts;
- * total order 1 or 2, order 2 for s and p shells only). */
+ * total order 1 to 4). */
 int qx_compute_2e_deriv(qx_handle *h, const int *deriv_vec, int len, double *out, int out_on_device,
                         void *stream);
 
@@ -145,8 +146,8 @@ int qx_class_info(const qx_handle *h, int cls, int *l4, long long *nquartets, lo
  * forms Hessians by jacfwd through eri_deriv_jvp, tei.py:342-346, over the order-2
  * tensor): Hv = sum_nu2 v_nu2 sum_ijkl Gamma_ijkl d2(ij|kl)/dR_nu1 dR_nu2 with
  * Gamma fixed (as in qx_grad_adjoint), one Hessian column per call for a unit v,
- * without the 3N(3N+1)/2 * n^4 tensor.  v and Hv hold 3N doubles.  This build:
- * s and p shells (QX_E_UNSUPPORTED otherwise). */
+ * without the 3N(3N+1)/2 * n^4 tensor.  v and Hv hold 3N doubles.  Every shell
+ * up to f. */
 int qx_grad_adjoint_jvp(qx_handle *h, const double *D, double cj, double ck, const double *v, double *Hv,
                         int on_device, void *stream);
 
@@ -221,6 +222,20 @@ int qx_autotune(qx_handle *h, int what, void *stream);
  * global accumulators + cooperative HRR, 5 warp VRR into global accumulators +
  * warp HRR), cfg[3] its warps per quartet. */
 int qx_engine_config(const qx_handle *h, int cls, int *cfg);
+
+/* Engine of one class chosen by the caller, no counterpart in the reference: the
+ * autotuner's choice made by hand, for tests and measurements.  plain / deriv are
+ * engine ids as qx_engine_config reports them (6 = Rys quadrature, available for
+ * every class), -1 keeps the current choice; pparam / dparam as in
+ * qx_engine_config.  QX_E_UNSUPPORTED when the class lacks the engine.
+ * Synchronises the device. */
+int qx_set_engine(qx_handle *h, int cls, int plain, int pparam, int deriv, int dparam);
+
+/* The canonical shell indices (s1, s2, s3, s4) of one class's screened unique
+ * quartets, in the order of the unique layout (shells[4*qi + i], host memory of
+ * 4 * nquartets ints).  No counterpart in the reference; lets a caller map the
+ * unique layout of qx_eri_unique back to shell quartets. */
+int qx_class_quartets(const qx_handle *h, int cls, int *shells);
 
 /* Size of the fixed device array qx_compute_2e_int_noalloc works in. */
 #define QX_NOALLOC_SCRATCH_BYTES (16u << 20)

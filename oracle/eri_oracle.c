@@ -947,7 +947,10 @@ int qxo_eri_deriv2(const qxo_basis *B, double thr, int pair_idx, double *out, in
     int nt = nthreads_of(nthreads);
 #pragma omp parallel num_threads(nt)
     {
-        double *buf = (double *)malloc(sizeof(double) * 1296 * 144);
+        int lmx = 0;
+        for (int s = 0; s < ns; ++s) lmx = B->l[s] > lmx ? B->l[s] : lmx;
+        size_t nb = (size_t)ncart(lmx) * ncart(lmx) * ncart(lmx) * ncart(lmx);
+        double *buf = (double *)malloc(sizeof(double) * nb * 144);
 #pragma omp for schedule(dynamic)
         for (int ip = 0; ip < np; ++ip) {
             int p1 = pairs[2 * ip], p2 = pairs[2 * ip + 1];

@@ -71,9 +71,12 @@ def _compile(src: str, hmt: float, verbose: bool):
 
 def build(verbose: bool = False, jobs: int | None = None) -> str:
     os.makedirs(BUILD, exist_ok=True)
-    gen_hdr = os.path.join(CSRC, "gen", "eri_classes.cuh")
-    if not os.path.exists(gen_hdr) or os.path.getmtime(gen_hdr) < os.path.getmtime(os.path.join(CSRC, "gen_eri.py")):
+    # the generator rewrites only files whose content changed; a stamp records the run
+    stamp = os.path.join(CSRC, "gen", ".stamp")
+    if not os.path.exists(stamp) or os.path.getmtime(stamp) < os.path.getmtime(os.path.join(CSRC, "gen_eri.py")):
         subprocess.run([sys.executable, os.path.join(CSRC, "gen_eri.py")], check=True)
+        with open(stamp, "w") as f:
+            f.write("generated\n")
     hmt = _headers_mtime()
     srcs = sources()
     with ThreadPoolExecutor(max_workers=jobs or os.cpu_count() or 4) as ex:

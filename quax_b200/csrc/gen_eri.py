@@ -1085,6 +1085,66 @@ def quartet_classes(lmax):
     return out
 
 
+class _Out:
+    """File writer that leaves an existing file untouched when its content is
+    unchanged, so a regeneration does not force the (slow) recompilation of
+    every generated translation unit."""
+
+    def __init__(self, path, mode="w"):
+        self.path, self.parts = path, []
+
+    def __enter__(self):
+        return self
+
+    def write(self, text):
+        self.parts.append(text)
+
+    def __exit__(self, *exc):
+        text = "".join(self.parts)
+        if os.path.exists(self.path):
+            with open(self.path) as f:
+                if f.read() == text:
+                    return
+        with open(self.path, "w") as f:
+            f.write(text)
+
+
+# Highest shell angular momentum of the Rys engine (every class up to (ff|ff)).
+RYS_LMAX = 3
+RYS_ALL_KINDS = ("RK_PLAIN", "RK_GRAD", "RK_HVP", "RK_DER1", "RK_DER2", "RK_DER3", "RK_DER4")
+
+
+def gen_rys(here, lmax_os):
+    """One translation unit per class up to RYS_LMAX with the Rys launcher
+    qx_launch_rys_<id>(args, kind, mode, nwork, stream) -> 0, or 1 when the kind
+    does not fit shared memory for the class.  Every class gets every kind: for
+    the f classes this is the only engine, for the l <= lmax_os classes it
+    serves the second- and higher-order derivatives and is an autotuner
+    candidate next to the Obara-Saika programs."""
+    del lmax_os
+    qc = quartet_classes(RYS_LMAX)
+    for i, (a, b, c, d) in enumerate(qc):
+        kinds = RYS_ALL_KINDS
+        L = ["// Generated by quax_b200/csrc/gen_eri.py -- do not edit by hand.",
+             f"// Rys-engine launchers of class ({a}{b}|{c}{d}).",
+             '#include "../qx_rys.cuh"',
+             f"int qx_launch_rys_{i:02d}(const qx::RysArgs& ra, int kind, int mode, long long nwork, cudaStream_t s) {{",
+             "    switch (kind) {"]
+        for k in kinds:
+            L.append(f"    case qx::{k}: return qx::launch_rys<{a}, {b}, {c}, {d}, qx::{k}>(ra, mode, nwork, s) ? 0 : 1;")
+        L += ["    default: return 1;", "    }", "}"]
+        with _Out(os.path.join(here, "gen", f"k_rys_{i:02d}.cu")) as f:
+            f.write("\n".join(L) + "\n")
+    H = ["// Generated by quax_b200/csrc/gen_eri.py -- do not edit by hand.", "#pragma once",
+         f"#define QX_RYS_LMAX {RYS_LMAX}",
+         f"#define QX_NCLS_ALL {len(qc)}",
+         f"#define QX_NPCLS_ALL {len(pair_classes(RYS_LMAX))}",
+         "// X(class_id, LA, LB, LC, LD) for every canonical class up to QX_RYS_LMAX",
+         "#define QX_FOR_EACH_CLASS_ALL(X) " + " ".join(f"X({i:02d}, {a}, {b}, {c}, {d})" for i, (a, b, c, d) in enumerate(qc))]
+    with _Out(os.path.join(here, "gen", "rys_index.cuh")) as f:
+        f.write("\n".join(H) + "\n")
+
+
 def main():
     lmax = int(sys.argv[1]) if len(sys.argv) > 1 else 2
     here = os.path.dirname(os.path.abspath(__file__))
@@ -1113,13 +1173,10 @@ def main():
     for k, name in enumerate(("VRR", "HRR", "DVRR", "DHRR")):
         hdr.append(f"#define QX_CLASS_{name}_FLOPS " + "{" + ", ".join(str(f[k]) for f in fl) + "}")
     body = [gen_plain(*c) for c in qc if c not in COOP_CLASSES]
-    with open(os.path.join(here, "gen", "coop_tables.cuh"), "w") as f:
+    with _Out(os.path.join(here, "gen", "coop_tables.cuh")) as f:
         f.write(gen_coop([(i, c) for i, c in enumerate(qc) if c in COOP_CLASSES]))
-    with open(os.path.join(here, "gen", "eri_classes.cuh"), "w") as f:
+    with _Out(os.path.join(here, "gen", "eri_classes.cuh")) as f:
         f.write("\n".join(hdr) + "\n\n" + "\n\n".join(body) + "\n")
-    for fn in os.listdir(os.path.join(here, "gen")):
-        if fn.startswith("k_eri_") and fn.endswith(".cu"):
-            os.remove(os.path.join(here, "gen", fn))
     wp, wd, wh, wv, wq = [], [], [], [], []
     for i, (a, b, c, d) in enumerate(qc):
         okp, pp = warp_feasible(a, b, c, d, 0)
@@ -1135,7 +1192,7 @@ def main():
         wv.append(okv)
         if (a, b, c, d) in COOP_CLASSES and not okp and not okd and not okv:
             continue
-        with open(os.path.join(here, "gen", f"k_eri_{i:02d}.cu"), "w") as f:
+        with _Out(os.path.join(here, "gen", f"k_eri_{i:02d}.cu")) as f:
             f.write("// Generated by quax_b200/csrc/gen_eri.py -- do not edit by hand.\n")
             f.write(f"// Kernels of class ({a}{b}|{c}{d}).\n")
             f.write('#include "../qx_warp.cuh"\n')
@@ -1148,7 +1205,7 @@ def main():
                 f.write(gen_warp_code(i, a, b, c, d, 1, pd, want_warp=okd, want_wvrr=okv) + "\n")
             if okh:
                 f.write(gen_warp_code(i, a, b, c, d, 2, ph) + "\n")
-    with open(os.path.join(here, "gen", "warp_index.cuh"), "w") as f:
+    with _Out(os.path.join(here, "gen", "warp_index.cuh")) as f:
         f.write("// Generated by quax_b200/csrc/gen_eri.py -- do not edit by hand.\n#pragma once\n")
         f.write("#define QX_CLASS_WARP_PLAIN {" + ", ".join("1" if x else "0" for x in wp) + "}\n")
         f.write("#define QX_CLASS_WARP_DERIV {" + ", ".join("1" if x else "0" for x in wd) + "}\n")
@@ -1163,8 +1220,9 @@ def main():
         f.write("#define QX_FOR_EACH_WVRR(X) " + " ".join(f"X({i:02d})" for i, x in enumerate(wv) if x) + "\n")
         f.write("#define QX_CLASS_WARP_DERIV2 {" + ", ".join("1" if x else "0" for x in wh) + "}\n")
         f.write("#define QX_FOR_EACH_WARP_DERIV2(X) " + " ".join(f"X({i:02d})" for i, x in enumerate(wh) if x) + "\n")
-    with open(os.path.join(here, "gen", "der_tables.cuh"), "w") as f:
+    with _Out(os.path.join(here, "gen", "der_tables.cuh")) as f:
         f.write(gen_coop_deriv(list(enumerate(qc))))
+    gen_rys(here, lmax)
 
 
 if __name__ == "__main__":

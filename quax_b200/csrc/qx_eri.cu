@@ -30,7 +30,9 @@
 
 #include "quax_b200.h"
 #include "qx_warp.cuh"
+#include "qx_rys.cuh"
 #include "gen/warp_index.cuh"
+#include "gen/rys_index.cuh"
 
 using namespace qx;
 
@@ -56,8 +58,8 @@ static int fail(int code, const char* fmt, ...) {
 
 extern "C" const char* qx_last_error(void) { return g_err.c_str(); }
 void qx_set_last_error(const char* msg) { g_err = msg; }
-extern "C" int qx_max_l(void) { return QX_GEN_LMAX; }
-extern "C" int qx_max_deriv_order(void) { return 2; }
+extern "C" int qx_max_l(void) { return QX_RYS_LMAX; }
+extern "C" int qx_max_deriv_order(void) { return 4; }
 
 static constexpr int pair_class(int l1, int l2) { return l1 * (l1 + 1) / 2 + l2; }
 static constexpr int quartet_class(int pb, int pk) { return pb * (pb + 1) / 2 + pk; }
@@ -77,33 +79,41 @@ struct DeviceGuard {
 
 // Per-class launch table: straight-line kernels where generated, the
 // warp-cooperative engine for the large classes.
-static EriLaunch g_eri_launch[QX_NUM_CLASSES];
-static long long g_class_scratch[QX_NUM_CLASSES];
-static const int g_class_nout[QX_NUM_CLASSES] = QX_CLASS_NOUT;
-static const int g_class_coop[QX_NUM_CLASSES] = QX_CLASS_COOP;
-static const long long g_class_vrr_flops[QX_NUM_CLASSES] = QX_CLASS_VRR_FLOPS;
-static const long long g_class_hrr_flops[QX_NUM_CLASSES] = QX_CLASS_HRR_FLOPS;
-static const long long g_class_dvrr_flops[QX_NUM_CLASSES] = QX_CLASS_DVRR_FLOPS;
-static const long long g_class_dhrr_flops[QX_NUM_CLASSES] = QX_CLASS_DHRR_FLOPS;
-static const int g_class_l[QX_NUM_CLASSES][4] = {
+static EriLaunch g_eri_launch[QX_NCLS_ALL];
+static long long g_class_scratch[QX_NCLS_ALL];
+static int g_class_nout[QX_NCLS_ALL];
+static const int g_class_coop[QX_NCLS_ALL] = QX_CLASS_COOP;
+static const long long g_class_vrr_flops[QX_NCLS_ALL] = QX_CLASS_VRR_FLOPS;
+static const long long g_class_hrr_flops[QX_NCLS_ALL] = QX_CLASS_HRR_FLOPS;
+static const long long g_class_dvrr_flops[QX_NCLS_ALL] = QX_CLASS_DVRR_FLOPS;
+static const long long g_class_dhrr_flops[QX_NCLS_ALL] = QX_CLASS_DHRR_FLOPS;
+static const int g_class_l[QX_NCLS_ALL][4] = {
 #define QX_L_ENTRY(id, a, b, c, d) {a, b, c, d},
-    QX_FOR_EACH_CLASS(QX_L_ENTRY)
+    QX_FOR_EACH_CLASS_ALL(QX_L_ENTRY)
 #undef QX_L_ENTRY
 };
-static int g_coop_idx[QX_NUM_CLASSES];
-static int g_der_idx[QX_NUM_CLASSES];
-static const int g_class_nacc[QX_NUM_CLASSES] = QX_CLASS_NACC;
-static const int g_has_warp_plain[QX_NUM_CLASSES] = QX_CLASS_WARP_PLAIN;
-static const int g_has_warp_deriv[QX_NUM_CLASSES] = QX_CLASS_WARP_DERIV;
-static const int g_has_wvrr[QX_NUM_CLASSES] = QX_CLASS_WVRR;
-static const int g_has_pvrr[QX_NUM_CLASSES] = QX_CLASS_PVRR;
-static const int g_has_dsplit[QX_NUM_CLASSES] = QX_CLASS_DSPLIT;
-static WarpLaunch g_warp_plain[QX_NUM_CLASSES];
-static WarpLaunch g_warp_deriv[QX_NUM_CLASSES];
-static WarpLaunch g_warp_deriv2[QX_NUM_CLASSES];  // second derivatives (classes with l <= 1)
-static WvrrLaunch g_wvrr[QX_NUM_CLASSES];          // derivative VRR into global accumulators
-static WvrrLaunch g_pvrr[QX_NUM_CLASSES];          // plain VRR into global accumulators
-static WvrrLaunch g_dsplit[QX_NUM_CLASSES];        // derivative VRR into item-order accumulators
+// Rys-engine launchers, one per class (gen/k_rys_<id>.cu): 0 = launched, 1 = this
+// kind is not compiled for the class or its tables exceed shared memory.
+typedef int (*RysLaunch)(const qx::RysArgs&, int kind, int mode, long long nwork, cudaStream_t);
+#define QX_DECL_RYS(id, a, b, c, d) int qx_launch_rys_##id(const qx::RysArgs&, int, int, long long, cudaStream_t);
+QX_FOR_EACH_CLASS_ALL(QX_DECL_RYS)
+#undef QX_DECL_RYS
+static RysLaunch g_rys_launch[QX_NCLS_ALL];
+const double* qx_rys_table();
+static int g_coop_idx[QX_NCLS_ALL];
+static int g_der_idx[QX_NCLS_ALL];
+static const int g_class_nacc[QX_NCLS_ALL] = QX_CLASS_NACC;
+static const int g_has_warp_plain[QX_NCLS_ALL] = QX_CLASS_WARP_PLAIN;
+static const int g_has_warp_deriv[QX_NCLS_ALL] = QX_CLASS_WARP_DERIV;
+static const int g_has_wvrr[QX_NCLS_ALL] = QX_CLASS_WVRR;
+static const int g_has_pvrr[QX_NCLS_ALL] = QX_CLASS_PVRR;
+static const int g_has_dsplit[QX_NCLS_ALL] = QX_CLASS_DSPLIT;
+static WarpLaunch g_warp_plain[QX_NCLS_ALL];
+static WarpLaunch g_warp_deriv[QX_NCLS_ALL];
+static WarpLaunch g_warp_deriv2[QX_NCLS_ALL];  // second derivatives (classes with l <= 1)
+static WvrrLaunch g_wvrr[QX_NCLS_ALL];          // derivative VRR into global accumulators
+static WvrrLaunch g_pvrr[QX_NCLS_ALL];          // plain VRR into global accumulators
+static WvrrLaunch g_dsplit[QX_NCLS_ALL];        // derivative VRR into item-order accumulators
 #define QX_DECL_WP(id) void qx_launch_warp_p##id(const qx::WarpArgs&, int, cudaStream_t);
 QX_FOR_EACH_WARP_PLAIN(QX_DECL_WP)
 #define QX_DECL_WD(id) void qx_launch_warp_d##id(const qx::WarpArgs&, int, cudaStream_t);
@@ -127,7 +137,9 @@ QX_FOR_EACH_DSPLIT(QX_DECL_DS)
 // cooperative HRR; ENG_WSPLIT (plain): the same VRR split + the warp HRR.
 // ENG_DSPLIT (derivatives): the split VRR into item-order accumulators + the warp
 // kernel's own HRR and epilogue.
-enum { ENG_SL = 0, ENG_WARP = 1, ENG_COOP = 2, ENG_WVRR = 3, ENG_WSPLIT = 4, ENG_DSPLIT = 5 };
+// ENG_RYS (plain and derivatives): the Rys-quadrature engine (qx_rys.cuh), the only
+// engine of the classes with an f shell.
+enum { ENG_SL = 0, ENG_WARP = 1, ENG_COOP = 2, ENG_WVRR = 3, ENG_WSPLIT = 4, ENG_DSPLIT = 5, ENG_RYS = 6 };
 int qx_der_index(int cls);
 void qx_launch_der_split(int der_idx, const qx::EriArgs& a, int mode, const double* D, double cj, double ck,
                          double* grad, int slice, const int2* tasks, long long ntask, double* scratch, cudaStream_t s);
@@ -139,12 +151,18 @@ void qx_launch_der(int der_idx, const qx::EriArgs& a, int mode, const double* D,
                    int slice, cudaStream_t s);
 enum { QX_MODE_DER_DENSE = 10, QX_MODE_DER_SLICE = 11, QX_MODE_GRAD = 12, QX_MODE_DER2_DENSE = 13,
        QX_MODE_DER2_SLICE = 14, QX_MODE_HVP = 15 };
+static bool has_os(int c) { return c < QX_NUM_CLASSES; }  // generated Obara-Saika programs (l <= 2)
 static bool init_class_tables() {
-    for (int c = 0; c < QX_NUM_CLASSES; ++c) {
+    static const int nout_os[QX_NUM_CLASSES] = QX_CLASS_NOUT;
+    for (int c = 0; c < QX_NCLS_ALL; ++c) {
         g_eri_launch[c] = nullptr;
         g_class_scratch[c] = 0;
-        g_coop_idx[c] = g_class_coop[c] ? qx_coop_index(c) : -1;
-        g_der_idx[c] = qx_der_index(c);
+        g_coop_idx[c] = has_os(c) && g_class_coop[c] ? qx_coop_index(c) : -1;
+        g_der_idx[c] = has_os(c) ? qx_der_index(c) : -1;
+        int nout = 1;
+        for (int i = 0; i < 4; ++i) nout *= (g_class_l[c][i] + 1) * (g_class_l[c][i] + 2) / 2;
+        g_class_nout[c] = nout;
+        if (has_os(c) && nout_os[c] != nout) return false;
         g_warp_plain[c] = nullptr;
         g_warp_deriv[c] = nullptr;
         g_warp_deriv2[c] = nullptr;
@@ -164,6 +182,9 @@ static bool init_class_tables() {
     QX_FOR_EACH_PVRR(QX_SET_PV)
 #define QX_SET_DS(id) g_dsplit[1##id - 100] = &qx_launch_dsplit_d##id;
     QX_FOR_EACH_DSPLIT(QX_SET_DS)
+#define QX_RYS_ENTRY(id, a, b, c, d) g_rys_launch[1##id - 100] = &qx_launch_rys_##id;
+    QX_FOR_EACH_CLASS_ALL(QX_RYS_ENTRY)
+#undef QX_RYS_ENTRY
 #define QX_SL_ENTRY(id, a, b, c, d)                            \
     g_eri_launch[id] = &qx_launch_eri_##id;                    \
     g_class_scratch[id] = qx::scratch_per_quartet<a, b, c, d>();
@@ -262,21 +283,22 @@ struct qx_handle {
     PrimPair* d_prims = nullptr;
     PairInfo* d_pairs = nullptr;
     double* d_boys = nullptr;
+    const double* d_rys = nullptr;  // Rys node/weight table (module data, not owned)
     int* d_err = nullptr;
     double* d_scratch = nullptr;  // accumulators of classes too large for shared memory
     long long scratch_len = 0;
     std::vector<double> K;  // nshell^2
     double kmax = 0.0;
-    ClassWork work[QX_NUM_CLASSES];
+    ClassWork work[QX_NCLS_ALL];
     long long nunique = 0, unique_size = 0;
     cudaStream_t streams[QX_NSTREAMS] = {};
     cudaEvent_t done[QX_NSTREAMS] = {};
     cudaEvent_t start = nullptr;
-    int order[QX_NUM_CLASSES];  // classes by decreasing primitive work
-    int plain_eng[QX_NUM_CLASSES];
-    int deriv_eng[QX_NUM_CLASSES];
-    int wpq[QX_NUM_CLASSES];        // warps per quartet, plain warp kernels
-    int wpq_deriv[QX_NUM_CLASSES];  // warps per quartet, derivative warp kernels
+    int order[QX_NCLS_ALL];  // classes by decreasing primitive work
+    int plain_eng[QX_NCLS_ALL];
+    int deriv_eng[QX_NCLS_ALL];
+    int wpq[QX_NCLS_ALL];        // warps per quartet, plain warp kernels
+    int wpq_deriv[QX_NCLS_ALL];  // warps per quartet, derivative warp kernels
     int shard_rank = 0, shard_n = 1;
     int prim_stage = 0;  // split-mode VRR: primitive pairs staged per warp (2 x largest pair), 0 = off
     // J/K density screening: sqrt(K) and max |D| per pair record, threshold of the
@@ -393,7 +415,11 @@ static int choose_wpq(long long nq, long long prims) {
 static void choose_engines(qx_handle* h) {
     const char* pe = std::getenv("QX_PLAIN_ENGINE");
     const char* de = std::getenv("QX_DERIV_ENGINE");
-    for (int c = 0; c < QX_NUM_CLASSES; ++c) {
+    for (int c = 0; c < QX_NCLS_ALL; ++c) {
+        if (!has_os(c)) {  // f shells: the Rys engine only
+            h->plain_eng[c] = h->deriv_eng[c] = ENG_RYS;
+            continue;
+        }
         int p;
         if (g_has_pvrr[c]) p = ENG_WSPLIT;  // measured fastest for these classes
         else if (g_has_warp_plain[c] && g_class_nacc[c] > 48) p = ENG_WARP;
@@ -478,7 +504,14 @@ static int run_class(qx_handle* h, int cls, int mode, const int2* d_q, long long
         a.jk_kpair = h->d_kpair;
         a.jk_dmax = h->d_dmax;
     }
-    if (eng == ENG_COOP) {
+    if (eng == ENG_RYS) {
+        RysArgs ra;
+        ra.e = a;
+        ra.rys = h->d_rys;
+        if (g_rys_launch[cls](ra, RK_PLAIN, mode, nq, s))
+            return fail(QX_E_UNSUPPORTED, "class (%d%d|%d%d): no Rys program", g_class_l[cls][0], g_class_l[cls][1],
+                        g_class_l[cls][2], g_class_l[cls][3]);
+    } else if (eng == ENG_COOP) {
         qx_launch_coop(g_coop_idx[cls], a, mode, s);
     } else if (eng == ENG_WARP || eng == ENG_WSPLIT) {
         WarpArgs wa;
@@ -544,7 +577,7 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
     qx_handle* h = new qx_handle();
     cudaGetDevice(&h->device);
     choose_engines(h);
-    for (int c = 0; c < QX_NUM_CLASSES; ++c) h->wpq[c] = h->wpq_deriv[c] = 1;
+    for (int c = 0; c < QX_NCLS_ALL; ++c) h->wpq[c] = h->wpq_deriv[c] = 1;
     h->natom = natom;
     h->nshell = nshell;
     h->pure = pure;
@@ -553,9 +586,9 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
     int off = 0, bf = 0;
     for (int s = 0; s < nshell; ++s) {
         const int l = shell_l[s], k = shell_nprim[s], at = shell_atom[s];
-        if (l < 0 || l > QX_GEN_LMAX) {
+        if (l < 0 || l > QX_RYS_LMAX) {
             free_handle(h);
-            return fail(QX_E_UNSUPPORTED, "qx_initialize: shell %d has l=%d (compiled max %d)", s, l, QX_GEN_LMAX);
+            return fail(QX_E_UNSUPPORTED, "qx_initialize: shell %d has l=%d (compiled max %d)", s, l, QX_RYS_LMAX);
         }
         if (k <= 0 || k > 64) {
             free_handle(h);
@@ -656,6 +689,11 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
                         (size_t)(bytes));                                             \
         }                                                                             \
     } while (0)
+    h->d_rys = qx_rys_table();
+    if (!h->d_rys) {
+        free_handle(h);
+        return fail(QX_E_CUDA, "qx_initialize: Rys table not found on device %d", h->device);
+    }
     QX_ALLOC(h->d_prims, sizeof(PrimPair) * prims.size());
     QX_ALLOC(h->d_pairs, sizeof(PairInfo) * np);
     QX_ALLOC(h->d_boys, sizeof(double) * boys.size());
@@ -667,7 +705,7 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
     // global accumulator scratch, sized for the largest launch that needs it
     {
         long long need = 0;
-        for (int c = 0; c < QX_NUM_CLASSES; ++c) need = std::max(need, g_class_scratch[c] * launch_threads(np, 0));
+        for (int c = 0; c < QX_NCLS_ALL; ++c) need = std::max(need, g_class_scratch[c] * launch_threads(np, 0));
         if (need) {
             QX_ALLOC(h->d_scratch, sizeof(double) * need);
             h->scratch_len = need;
@@ -675,14 +713,14 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
     }
     // Schwarz: diagonal quartets (P|P) of every pair
     {
-        std::vector<std::vector<int2>> diag(QX_NUM_PAIR_CLASSES);
+        std::vector<std::vector<int2>> diag(QX_NPCLS_ALL);
         for (int p = 0; p < np; ++p) diag[h->pcls[p]].push_back(make_int2(p, p));
         double* d_kp = nullptr;
         int2* d_dq = nullptr;
         QX_ALLOC(d_kp, sizeof(double) * np);
         QX_ALLOC(d_dq, sizeof(int2) * np);
         long long o = 0;
-        for (int pc = 0; pc < QX_NUM_PAIR_CLASSES; ++pc) {
+        for (int pc = 0; pc < QX_NPCLS_ALL; ++pc) {
             if (diag[pc].empty()) continue;
             cudaMemcpy(d_dq + o, diag[pc].data(), sizeof(int2) * diag[pc].size(), cudaMemcpyHostToDevice);
             // few quartets with long primitive loops: 32 lanes (straight-line kernels
@@ -749,40 +787,40 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
                 fn(quartet_class(h->pcls[pb], h->pcls[pk]), key(pb, pk), pb, pk);
             }
     };
-    std::vector<long long> cnt((size_t)nt * QX_NUM_CLASSES * NKEY, 0);
-    std::vector<long long> tprims((size_t)nt * QX_NUM_CLASSES, 0);
+    std::vector<long long> cnt((size_t)nt * QX_NCLS_ALL * NKEY, 0);
+    std::vector<long long> tprims((size_t)nt * QX_NCLS_ALL, 0);
     host_parallel(nt, [&](int t) {
-        long long* C = cnt.data() + (size_t)t * QX_NUM_CLASSES * NKEY;
-        long long* P = tprims.data() + (size_t)t * QX_NUM_CLASSES;
+        long long* C = cnt.data() + (size_t)t * QX_NCLS_ALL * NKEY;
+        long long* P = tprims.data() + (size_t)t * QX_NCLS_ALL;
         visit(t, [&](int c, int k, int pb, int pk) {
             C[(size_t)c * NKEY + k]++;
             P[c] += (long long)h->pairs[pb].nprim * h->pairs[pk].nprim;
         });
     });
-    std::vector<long long> nq_c(QX_NUM_CLASSES, 0), prims_c(QX_NUM_CLASSES, 0);
-    for (int c = 0; c < QX_NUM_CLASSES; ++c) {
+    std::vector<long long> nq_c(QX_NCLS_ALL, 0), prims_c(QX_NCLS_ALL, 0);
+    for (int c = 0; c < QX_NCLS_ALL; ++c) {
         long long run = 0;
         for (int k = 0; k < NKEY; ++k)
             for (int t = 0; t < nt; ++t) {
-                long long& x = cnt[((size_t)t * QX_NUM_CLASSES + c) * NKEY + k];
+                long long& x = cnt[((size_t)t * QX_NCLS_ALL + c) * NKEY + k];
                 const long long v = x;
                 x = run;
                 run += v;
             }
         nq_c[c] = run;
-        for (int t = 0; t < nt; ++t) prims_c[c] += tprims[(size_t)t * QX_NUM_CLASSES + c];
+        for (int t = 0; t < nt; ++t) prims_c[c] += tprims[(size_t)t * QX_NCLS_ALL + c];
     }
-    std::vector<std::unique_ptr<int2[]>> sorted(QX_NUM_CLASSES);
-    for (int c = 0; c < QX_NUM_CLASSES; ++c)
+    std::vector<std::unique_ptr<int2[]>> sorted(QX_NCLS_ALL);
+    for (int c = 0; c < QX_NCLS_ALL; ++c)
         if (nq_c[c]) sorted[c].reset(new int2[(size_t)nq_c[c]]);
     host_parallel(nt, [&](int t) {
-        long long* C = cnt.data() + (size_t)t * QX_NUM_CLASSES * NKEY;
+        long long* C = cnt.data() + (size_t)t * QX_NCLS_ALL * NKEY;
         visit(t, [&](int c, int k, int pb, int pk) { sorted[c][C[(size_t)c * NKEY + k]++] = make_int2(pb, pk); });
     });
     std::vector<long long>().swap(cnt);
     trace.mark("quartet enumeration, sort");
     long long base = 0;
-    for (int c = 0; c < QX_NUM_CLASSES; ++c) {
+    for (int c = 0; c < QX_NCLS_ALL; ++c) {
         ClassWork& w = h->work[c];
         w.nq = nq_c[c];
         w.prims = prims_c[c];
@@ -810,8 +848,8 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
     }
     h->unique_size = base;
     trace.mark("list uploads, split tasks");
-    for (int c = 0; c < QX_NUM_CLASSES; ++c) h->order[c] = c;
-    std::sort(h->order, h->order + QX_NUM_CLASSES,
+    for (int c = 0; c < QX_NCLS_ALL; ++c) h->order[c] = c;
+    std::sort(h->order, h->order + QX_NCLS_ALL,
               [&](int x, int y) { return h->work[x].prims * g_class_nout[x] > h->work[y].prims * g_class_nout[y]; });
     for (int i = 0; i < QX_NSTREAMS; ++i) {
         if (cudaStreamCreateWithFlags(&h->streams[i], cudaStreamNonBlocking) != cudaSuccess ||
@@ -869,7 +907,7 @@ static int rebuild_views(qx_handle* h) {
     const int rank = h->shard_rank, nranks = h->shard_n;
     long long base = 0;
     h->nunique = 0;
-    for (int c = 0; c < QX_NUM_CLASSES; ++c) {
+    for (int c = 0; c < QX_NCLS_ALL; ++c) {
         ClassWork& w = h->work[c];
         cudaFree(w.d_dtasks);
         cudaFree(w.d_dacc);
@@ -933,7 +971,7 @@ extern "C" int qx_set_precision(qx_handle* h, double bound) {
     const double b2 = h->f32_bound * h->f32_bound;
     const int ns = h->nshell;
     auto kpair = [&](const PairInfo& p) { return h->K[(size_t)p.s1 * ns + p.s2]; };
-    for (int c = 0; c < QX_NUM_CLASSES; ++c) {
+    for (int c = 0; c < QX_NCLS_ALL; ++c) {
         ClassWork& w = h->work[c];
         if (!w.nq_full) continue;
         std::vector<int2> L((size_t)w.nq_full);
@@ -946,7 +984,7 @@ extern "C" int qx_set_precision(qx_handle* h, double bound) {
         // tenfold per transfer step (measured relative error of the FP32 path:
         // <= 4e-5 with lb + ld <= 1, ~2e-3 with 2, 1e-1 with 3, above 1 with 4), so
         // classes with more than two transfer steps stay FP64
-        const bool eligible = g_class_l[c][1] + g_class_l[c][3] <= 2;
+        const bool eligible = has_os(c) && g_class_l[c][1] + g_class_l[c][3] <= 2;
         auto is64 = [&](const int2& q) {
             return !eligible || b2 <= 0.0 || kpair(h->pairs[q.x]) * kpair(h->pairs[q.y]) >= b2;
         };
@@ -959,7 +997,7 @@ extern "C" int qx_set_precision(qx_handle* h, double bound) {
 }
 
 extern "C" long long qx_precision_split(const qx_handle* h, int cls) {
-    if (!h || cls < 0 || cls >= QX_NUM_CLASSES) return fail(QX_E_INVALID, "qx_precision_split: bad argument");
+    if (!h || cls < 0 || cls >= QX_NCLS_ALL) return fail(QX_E_INVALID, "qx_precision_split: bad argument");
     const ClassWork& w = h->work[cls];
     return w.nq64 >= w.nq ? w.nq : w.nq64;
 }
@@ -1002,7 +1040,7 @@ static int run_all_classes(qx_handle* h, int mode, double* out, long long n, cud
     QX_CUDA(cudaEventRecord(h->start, s));
     for (int i = 0; i < QX_NSTREAMS; ++i) QX_CUDA(cudaStreamWaitEvent(h->streams[i], h->start, 0));
     int k = 0;
-    for (int oi = 0; oi < QX_NUM_CLASSES; ++oi) {
+    for (int oi = 0; oi < QX_NCLS_ALL; ++oi) {
         const int c = h->order[oi];
         const ClassWork& w = h->work[c];
         if (!w.nq) continue;
@@ -1073,9 +1111,67 @@ static EriArgs class_args(qx_handle* h, int c, double* out) {
     return a;
 }
 
+static long long binom_ll(int n, int k) {
+    long long r = 1;
+    for (int i = 1; i <= k; ++i) r = r * (n - k + i) / i;
+    return r;
+}
+
+static int rys_unsupported(int c, const char* what) {
+    return fail(QX_E_UNSUPPORTED, "class (%d%d|%d%d): the Rys %s program does not fit shared memory or is not compiled",
+                g_class_l[c][0], g_class_l[c][1], g_class_l[c][2], g_class_l[c][3], what);
+}
+
+// Derivative tensor of order k (1..4) of one class through the Rys engine:
+// dense (nu == nullptr; slot = the reference's rank of the sorted nuclear indices
+// over M = 3N) or the one slice of the sorted nuclear indices nu[0..k).
+static int run_rys_derk(qx_handle* h, int c, int k, double* out, const int* nu, cudaStream_t cs) {
+    const ClassWork& w = h->work[c];
+    if (!w.nq) return QX_OK;
+    RysArgs ra;
+    ra.e = class_args(h, c, out);
+    ra.rys = h->d_rys;
+    ra.M = 3 * h->natom;
+    const int nm = (int)binom_ll(11 + k, k);  // multisets of k of the 12 centre-directions
+    ra.chunk = std::min(nm, RYS_CHMAX);
+    ra.nchunk = (nm + ra.chunk - 1) / ra.chunk;
+    if (nu) {
+        ra.slice_k = k;
+        for (int i = 0; i < k; ++i) ra.slice_nu[i] = nu[i];
+    }
+    if (g_rys_launch[c](ra, RK_DER1 + k - 1, 0, w.nq * ra.nchunk, cs)) return rys_unsupported(c, "derivative");
+    QX_CUDA(cudaGetLastError());
+    return QX_OK;
+}
+
+// Adjoint gradient (kind RK_GRAD) or Hessian-vector product (RK_HVP) of one
+// class through the Rys engine.
+static int run_rys_contract(qx_handle* h, int c, int kind, const double* D, double cj, double ck, double* grad,
+                            const double* dir, cudaStream_t cs) {
+    const ClassWork& w = h->work[c];
+    if (!w.nq) return QX_OK;
+    RysArgs ra;
+    ra.e = class_args(h, c, nullptr);
+    ra.rys = h->d_rys;
+    ra.D = D;
+    ra.cj = cj;
+    ra.ck = ck;
+    ra.grad = grad;
+    ra.dir = dir;
+    ra.M = 3 * h->natom;
+    if (g_rys_launch[c](ra, kind, 0, w.nq, cs)) return rys_unsupported(c, kind == RK_GRAD ? "gradient" : "Hessian");
+    QX_CUDA(cudaGetLastError());
+    return QX_OK;
+}
+
 // One class through its first-derivative engine on stream `cs`.
 static int run_deriv_class(qx_handle* h, int c, int mode, double* out, const double* D, double cj, double ck,
                            double* grad, int slice, cudaStream_t cs) {
+    if (h->deriv_eng[c] == ENG_RYS) {
+        if (mode == QX_MODE_GRAD) return run_rys_contract(h, c, RK_GRAD, D, cj, ck, grad, nullptr, cs);
+        if (mode == QX_MODE_DER_DENSE) return run_rys_derk(h, c, 1, out, nullptr, cs);
+        return run_rys_derk(h, c, 1, out, &slice, cs);
+    }
     if (h->deriv_eng[c] == ENG_WARP) {
         WarpArgs wa;
         wa.e = class_args(h, c, out);
@@ -1139,7 +1235,7 @@ static int run_all_deriv(qx_handle* h, int mode, double* out, const double* D, d
     QX_CUDA(cudaEventRecord(h->start, s));
     for (int i = 0; i < QX_NSTREAMS; ++i) QX_CUDA(cudaStreamWaitEvent(h->streams[i], h->start, 0));
     int k = 0;
-    for (int oi = 0; oi < QX_NUM_CLASSES; ++oi) {
+    for (int oi = 0; oi < QX_NCLS_ALL; ++oi) {
         const int c = h->order[oi];
         if (!h->work[c].nq) continue;
         int rc = run_deriv_class(h, c, mode, out, D, cj, ck, grad, slice, h->streams[k++ % QX_NSTREAMS]);
@@ -1156,18 +1252,26 @@ static int run_all_deriv(qx_handle* h, int mode, double* out, const double* D, d
 // 3N for the dense tensor, or the packed nuclear pair nu1 | nu2 << 16 (nu1 <= nu2).
 static int run_all_deriv2(qx_handle* h, int mode, double* out, int slice, cudaStream_t s, const double* D = nullptr,
                           double cj = 0.0, double ck = 0.0, double* hv = nullptr, const double* dir = nullptr) {
-    for (int c = 0; c < QX_NUM_CLASSES; ++c)
-        if (h->work[c].nq && !g_warp_deriv2[c])
-            return fail(QX_E_UNSUPPORTED,
-                        "second derivatives: class (%d%d|%d%d) has no order-2 program (this build: s and p shells)",
-                        g_class_l[c][0], g_class_l[c][1], g_class_l[c][2], g_class_l[c][3]);
     QX_CUDA(cudaEventRecord(h->start, s));
     for (int i = 0; i < QX_NSTREAMS; ++i) QX_CUDA(cudaStreamWaitEvent(h->streams[i], h->start, 0));
     int k = 0;
-    for (int oi = 0; oi < QX_NUM_CLASSES; ++oi) {
+    for (int oi = 0; oi < QX_NCLS_ALL; ++oi) {
         const int c = h->order[oi];
         if (!h->work[c].nq) continue;
         cudaStream_t cs = h->streams[k++ % QX_NSTREAMS];
+        if (!g_warp_deriv2[c]) {  // classes with d or f shells: the Rys engine
+            int rc;
+            if (mode == QX_MODE_HVP) {
+                rc = run_rys_contract(h, c, RK_HVP, D, cj, ck, hv, dir, cs);
+            } else if (mode == QX_MODE_DER2_DENSE) {
+                rc = run_rys_derk(h, c, 2, out, nullptr, cs);
+            } else {
+                const int nu[2] = {slice & 0xffff, slice >> 16};
+                rc = run_rys_derk(h, c, 2, out, nu, cs);
+            }
+            if (rc) return rc;
+            continue;
+        }
         WarpArgs wa;
         wa.e = class_args(h, c, out);
         wa.wpq = h->wpq_deriv[c];
@@ -1179,6 +1283,25 @@ static int run_all_deriv2(qx_handle* h, int mode, double* out, int slice, cudaSt
         wa.dir = dir;
         g_warp_deriv2[c](wa, mode, cs);
         QX_CUDA(cudaGetLastError());
+    }
+    for (int i = 0; i < QX_NSTREAMS; ++i) {
+        QX_CUDA(cudaEventRecord(h->done[i], h->streams[i]));
+        QX_CUDA(cudaStreamWaitEvent(s, h->done[i], 0));
+    }
+    return QX_OK;
+}
+
+// Derivative tensors of order 3 or 4: every class through the Rys engine on the
+// internal streams (dense when nu == nullptr, else the slice nu[0..k)).
+static int run_all_derk(qx_handle* h, int k, double* out, const int* nu, cudaStream_t s) {
+    QX_CUDA(cudaEventRecord(h->start, s));
+    for (int i = 0; i < QX_NSTREAMS; ++i) QX_CUDA(cudaStreamWaitEvent(h->streams[i], h->start, 0));
+    int j = 0;
+    for (int oi = 0; oi < QX_NCLS_ALL; ++oi) {
+        const int c = h->order[oi];
+        if (!h->work[c].nq) continue;
+        int rc = run_rys_derk(h, c, k, out, nu, h->streams[j++ % QX_NSTREAMS]);
+        if (rc) return rc;
     }
     for (int i = 0; i < QX_NSTREAMS; ++i) {
         QX_CUDA(cudaEventRecord(h->done[i], h->streams[i]));
@@ -1209,15 +1332,16 @@ static int with_output(qx_handle* h, double* out, size_t count, int out_on_devic
 
 extern "C" int qx_eri_deriv_core(qx_handle* h, int order, double* out, int out_on_device, void* stream) {
     if (!h || !out) return fail(QX_E_INVALID, "qx_eri_deriv_core: NULL argument");
-    if (order < 1 || order > 2)
-        return fail(QX_E_UNSUPPORTED, "qx_eri_deriv_core: derivative order %d (this build: 1 and 2)", order);
+    if (order < 1 || order > 4)
+        return fail(QX_E_UNSUPPORTED, "qx_eri_deriv_core: derivative order %d (this build: 1 to 4)", order);
     DeviceGuard g(h->device);
     cudaStream_t s = (cudaStream_t)stream;
     const long long n = h->nbf, n4 = n * n * n * n;
     const long long M = 3LL * h->natom;
-    const size_t count = (size_t)(order == 1 ? M : M * (M + 1) / 2) * (size_t)n4;
+    const size_t count = (size_t)binom_ll((int)M + order - 1, order) * (size_t)n4;
     return with_output(h, out, count, out_on_device, s, [&](double* d) {
         QX_CUDA(cudaMemsetAsync(d, 0, sizeof(double) * count, s));
+        if (order >= 3) return run_all_derk(h, order, d, nullptr, s);
         if (order == 2) return run_all_deriv2(h, QX_MODE_DER2_DENSE, d, (int)M, s);
         return run_all_deriv(h, QX_MODE_DER_DENSE, d, nullptr, 0.0, 0.0, nullptr, -1, s);
     });
@@ -1229,20 +1353,22 @@ extern "C" int qx_compute_2e_deriv(qx_handle* h, const int* deriv_vec, int len, 
     if (len != 3 * h->natom)
         return fail(QX_E_INVALID, "qx_compute_2e_deriv: deriv_vec has %d entries, expected 3*natom = %d", len,
                     3 * h->natom);
-    int order = 0, nu[2] = {-1, -1};
+    int order = 0, nu[4] = {-1, -1, -1, -1};
     for (int i = 0; i < len; ++i) {
         if (deriv_vec[i] < 0) return fail(QX_E_INVALID, "qx_compute_2e_deriv: negative entry in deriv_vec");
-        for (int r = 0; r < deriv_vec[i] && order + r < 2; ++r) nu[order + r] = i;
+        if (deriv_vec[i] > 4) return fail(QX_E_UNSUPPORTED, "qx_compute_2e_deriv: derivative order above 4");
+        for (int r = 0; r < deriv_vec[i] && order + r < 4; ++r) nu[order + r] = i;
         order += deriv_vec[i];
     }
-    if (order < 1 || order > 2)
-        return fail(QX_E_UNSUPPORTED, "qx_compute_2e_deriv: derivative order %d (this build: 1 and 2)", order);
+    if (order < 1 || order > 4)
+        return fail(QX_E_UNSUPPORTED, "qx_compute_2e_deriv: derivative order %d (this build: 1 to 4)", order);
     if (order == 2 && len > 0xffff) return fail(QX_E_INVALID, "qx_compute_2e_deriv: too many atoms for order 2");
     DeviceGuard g(h->device);
     cudaStream_t s = (cudaStream_t)stream;
     const long long n = h->nbf, n4 = n * n * n * n;
     return with_output(h, out, (size_t)n4, out_on_device, s, [&](double* d) {
         QX_CUDA(cudaMemsetAsync(d, 0, sizeof(double) * n4, s));
+        if (order >= 3) return run_all_derk(h, order, d, nu, s);
         if (order == 2) return run_all_deriv2(h, QX_MODE_DER2_SLICE, d, nu[0] | nu[1] << 16, s);
         return run_all_deriv(h, QX_MODE_DER_SLICE, d, nullptr, 0.0, 0.0, nullptr, nu[0], s);
     });
@@ -1373,23 +1499,51 @@ extern "C" int qx_oei_deriv_core(qx_handle* h, int order, double* dS, double* dT
 }
 
 // ---------------------------------------------------------------- class info ---
-extern "C" int qx_num_classes(void) { return QX_NUM_CLASSES; }
+// Algorithmic FP64 FLOPs of one primitive quartet of the Rys programs (plain:
+// deriv = 0; adjoint gradient: deriv = 1), counted per step of qx_rys.cuh: the
+// 2n Chebyshev series (13 Clenshaw steps, 4 flops each), the 3n two-dimensional
+// tables (5 flops per entry), the transfer levels (2 per entry), the gradient's
+// four derivative tables (3 per entry) and the products (plain: 3 per component
+// and root; gradient: 22).
+static double rys_prim_flops(const int* l, int deriv) {
+    const int L = l[0] + l[1] + l[2] + l[3];
+    const int A1 = l[0] + 1 + deriv, B1 = l[1] + 1 + deriv, C1 = l[2] + 1 + deriv, D1 = l[3] + 1;
+    const int NI = A1 + B1 - 1, NK = C1 + D1 - 1, NR = (L + deriv) / 2 + 1;
+    double ncomp = 1.0, sz0 = 1.0;
+    for (int i = 0; i < 4; ++i) {
+        ncomp *= (l[i] + 1) * (l[i] + 2) / 2;
+        sz0 *= l[i] + 1;
+    }
+    double f = 2.0 * NR * 52.0 + 3.0 * NR * NI * NK * 5.0;
+    for (int b = 1; b < B1; ++b) f += 3.0 * NR * (NI - b) * NK * 2.0;
+    for (int d = 1; d < D1; ++d) f += 3.0 * NR * A1 * B1 * (NK - d) * 2.0;
+    if (deriv) f += 3.0 * NR * 4.0 * sz0 * 3.0 + ncomp * NR * 22.0;
+    else f += ncomp * NR * 3.0;
+    return f;
+}
+
+extern "C" int qx_num_classes(void) { return QX_NCLS_ALL; }
 
 extern "C" int qx_class_info(const qx_handle* h, int cls, int* l4, long long* nquartets, long long* nprim_quartets,
                              double* flops, double* flops_deriv) {
-    if (!h || cls < 0 || cls >= QX_NUM_CLASSES) return fail(QX_E_INVALID, "qx_class_info: bad handle or class");
+    if (!h || cls < 0 || cls >= QX_NCLS_ALL) return fail(QX_E_INVALID, "qx_class_info: bad handle or class");
     const ClassWork& w = h->work[cls];
     if (l4)
         for (int i = 0; i < 4; ++i) l4[i] = g_class_l[cls][i];
     if (nquartets) *nquartets = w.nq;
     if (nprim_quartets) *nprim_quartets = w.prims;
+    if (!has_os(cls)) {
+        if (flops) *flops = (double)w.prims * rys_prim_flops(g_class_l[cls], 0);
+        if (flops_deriv) *flops_deriv = (double)w.prims * rys_prim_flops(g_class_l[cls], 1);
+        return QX_OK;
+    }
     if (flops) *flops = (double)w.prims * g_class_vrr_flops[cls] + (double)w.nq * g_class_hrr_flops[cls];
     if (flops_deriv) *flops_deriv = (double)w.prims * g_class_dvrr_flops[cls] + (double)w.nq * g_class_dhrr_flops[cls];
     return QX_OK;
 }
 
 extern "C" int qx_eri_unique_class(qx_handle* h, int cls, double* out_dev, void* stream) {
-    if (!h || !out_dev || cls < 0 || cls >= QX_NUM_CLASSES) return fail(QX_E_INVALID, "qx_eri_unique_class: bad argument");
+    if (!h || !out_dev || cls < 0 || cls >= QX_NCLS_ALL) return fail(QX_E_INVALID, "qx_eri_unique_class: bad argument");
     DeviceGuard g(h->device);
     const ClassWork& w = h->work[cls];
     if (!w.nq) return QX_OK;
@@ -1399,7 +1553,7 @@ extern "C" int qx_eri_unique_class(qx_handle* h, int cls, double* out_dev, void*
 
 extern "C" int qx_grad_adjoint_class(qx_handle* h, int cls, const double* D_dev, double cj, double ck,
                                      double* grad_dev, void* stream) {
-    if (!h || !D_dev || !grad_dev || cls < 0 || cls >= QX_NUM_CLASSES)
+    if (!h || !D_dev || !grad_dev || cls < 0 || cls >= QX_NCLS_ALL)
         return fail(QX_E_INVALID, "qx_grad_adjoint_class: bad argument");
     DeviceGuard g(h->device);
     if (!h->work[cls].nq) return QX_OK;
@@ -1443,7 +1597,7 @@ extern "C" int qx_autotune(qx_handle* h, int what, void* stream) {
     DeviceGuard g(h->device);
     cudaStream_t s = (cudaStream_t)stream;
     long long max_out = 0;
-    for (int c = 0; c < QX_NUM_CLASSES; ++c) max_out = std::max(max_out, h->work[c].nq * (long long)g_class_nout[c]);
+    for (int c = 0; c < QX_NCLS_ALL; ++c) max_out = std::max(max_out, h->work[c].nq * (long long)g_class_nout[c]);
     const long long n = h->nbf;
     double *d_out = nullptr, *d_D = nullptr, *d_g = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -1461,9 +1615,9 @@ extern "C" int qx_autotune(qx_handle* h, int what, void* stream) {
         rc = fail(QX_E_CUDA, "qx_autotune: memset failed");
     if (!rc && cudaMemsetAsync(d_g, 0, sizeof(double) * 3 * h->natom, s) != cudaSuccess)
         rc = fail(QX_E_CUDA, "qx_autotune: memset failed");
-    for (int c = 0; c < QX_NUM_CLASSES && !rc; ++c) {
+    for (int c = 0; c < QX_NCLS_ALL && !rc; ++c) {
         ClassWork& w = h->work[c];
-        if (!w.nq) continue;
+        if (!w.nq || !has_os(c)) continue;  // the Rys classes have one engine
         if (what & 1) {
             std::vector<TuneCfg> cand;
             if (!g_class_coop[c] && !g_class_scratch[c])
@@ -1475,6 +1629,7 @@ extern "C" int qx_autotune(qx_handle* h, int what, void* stream) {
             if (g_class_coop[c]) cand.push_back({ENG_COOP, 0});
             if (g_has_pvrr[c] && g_has_warp_plain[c] && !ensure_split_tasks(h, c) && w.slice_q.size() == 2)
                 cand.push_back({ENG_WSPLIT, 1});
+            cand.push_back({ENG_RYS, 0});
             const int keep_wpq = h->wpq[c], keep_lg = w.log2g;
             float best = 1e30f;
             TuneCfg bc{h->plain_eng[c], h->plain_eng[c] == ENG_SL ? keep_lg : keep_wpq};
@@ -1505,6 +1660,7 @@ extern "C" int qx_autotune(qx_handle* h, int what, void* stream) {
             if (g_has_wvrr[c]) cand.push_back({ENG_WVRR, 0});
             if (g_has_dsplit[c]) cand.push_back({ENG_DSPLIT, 0});
             if (g_der_idx[c] >= 0) cand.push_back({ENG_COOP, 0});
+            cand.push_back({ENG_RYS, 0});
             float best = 1e30f;
             TuneCfg bc{h->deriv_eng[c], h->wpq_deriv[c]};
             for (const TuneCfg& t : cand) {
@@ -1537,8 +1693,83 @@ extern "C" int qx_autotune(qx_handle* h, int what, void* stream) {
     return rc;
 }
 
+// Engine of one class chosen by the caller (tests, measurements): the autotuner's
+// choice made by hand.  plain / deriv: engine ids as qx_engine_config reports
+// them, -1 keeps the current one; pparam / dparam: log2 lanes per quartet
+// (straight-line) or warps per quartet (warp kernels), ignored otherwise.
+extern "C" int qx_set_engine(qx_handle* h, int cls, int plain, int pparam, int deriv, int dparam) {
+    if (!h || cls < 0 || cls >= QX_NCLS_ALL) return fail(QX_E_INVALID, "qx_set_engine: bad handle or class");
+    DeviceGuard g(h->device);
+    ClassWork& w = h->work[cls];
+    const int* L = g_class_l[cls];
+    auto no = [&](const char* what, int e) {
+        return fail(QX_E_UNSUPPORTED, "qx_set_engine: class (%d%d|%d%d) has no %s engine %d", L[0], L[1], L[2], L[3],
+                    what, e);
+    };
+    if (plain >= 0) {
+        bool ok = false;
+        if (plain == ENG_SL) ok = has_os(cls) && !g_class_coop[cls] && pparam >= 0 && pparam <= 5;
+        if (plain == ENG_WARP) ok = has_os(cls) && g_has_warp_plain[cls] && (pparam == 1 || pparam == 4);
+        if (plain == ENG_COOP) ok = has_os(cls) && g_class_coop[cls];
+        if (plain == ENG_WSPLIT) ok = has_os(cls) && g_has_pvrr[cls] && g_has_warp_plain[cls];
+        if (plain == ENG_RYS) ok = true;
+        if (!ok) return no("plain", plain);
+        QX_CUDA(cudaDeviceSynchronize());
+        if (plain == ENG_SL && g_class_scratch[cls] && w.nq) {  // global accumulators for this lane count
+            cudaFree(w.scratch);
+            w.scratch = nullptr;
+            if (cudaMalloc((void**)&w.scratch, sizeof(double) * g_class_scratch[cls] * launch_threads(w.nq, pparam)) !=
+                cudaSuccess) {
+                cudaGetLastError();
+                w.scratch = nullptr;
+                return fail(QX_E_NOMEM, "qx_set_engine: accumulators for class %d", cls);
+            }
+        }
+        if (plain == ENG_WSPLIT) {
+            int rc = ensure_split_tasks(h, cls);
+            if (rc) return rc;
+        }
+        h->plain_eng[cls] = plain;
+        if (plain == ENG_SL) w.log2g = pparam;
+        if (plain == ENG_WARP) h->wpq[cls] = pparam;
+        if (plain == ENG_WSPLIT) h->wpq[cls] = 1;
+    }
+    if (deriv >= 0) {
+        bool ok = false;
+        if (deriv == ENG_WARP) ok = has_os(cls) && g_has_warp_deriv[cls] && (dparam == 1 || dparam == 4);
+        if (deriv == ENG_WVRR) ok = has_os(cls) && g_has_wvrr[cls];
+        if (deriv == ENG_DSPLIT) ok = has_os(cls) && g_has_dsplit[cls];
+        if (deriv == ENG_COOP) ok = g_der_idx[cls] >= 0;
+        if (deriv == ENG_RYS) ok = true;
+        if (!ok) return no("derivative", deriv);
+        h->deriv_eng[cls] = deriv;
+        if (deriv == ENG_WARP) h->wpq_deriv[cls] = dparam;
+    }
+    return QX_OK;
+}
+
+// The canonical shells of a class's quartets in this handle's list order (the
+// order of the unique layout): shells[4 * qi + 0..3] = (s1 s2|s3 s4).
+extern "C" int qx_class_quartets(const qx_handle* h, int cls, int* shells) {
+    if (!h || !shells || cls < 0 || cls >= QX_NCLS_ALL) return fail(QX_E_INVALID, "qx_class_quartets: bad argument");
+    DeviceGuard g(h->device);
+    const ClassWork& w = h->work[cls];
+    if (!w.nq) return QX_OK;
+    std::vector<int2> L((size_t)w.nq);
+    QX_CUDA(cudaMemcpy(L.data(), w.d_q, sizeof(int2) * w.nq, cudaMemcpyDeviceToHost));
+    for (long long i = 0; i < w.nq; ++i) {
+        const PairInfo& P = h->pairs[L[i].x];
+        const PairInfo& Q = h->pairs[L[i].y];
+        shells[4 * i + 0] = P.s1;
+        shells[4 * i + 1] = P.s2;
+        shells[4 * i + 2] = Q.s1;
+        shells[4 * i + 3] = Q.s2;
+    }
+    return QX_OK;
+}
+
 extern "C" int qx_engine_config(const qx_handle* h, int cls, int* cfg) {
-    if (!h || !cfg || cls < 0 || cls >= QX_NUM_CLASSES) return fail(QX_E_INVALID, "qx_engine_config: bad argument");
+    if (!h || !cfg || cls < 0 || cls >= QX_NCLS_ALL) return fail(QX_E_INVALID, "qx_engine_config: bad argument");
     cfg[0] = h->plain_eng[cls];
     cfg[1] = h->plain_eng[cls] == ENG_SL ? h->work[cls].log2g : (h->plain_eng[cls] == ENG_WARP ? h->wpq[cls] : 0);
     cfg[2] = h->deriv_eng[cls];

@@ -64,6 +64,8 @@ SIGNATURES = {
     "qx_precision_split": (C.c_longlong, [_vp, C.c_int]),
     "qx_partition_costs": (C.c_int, [_vp, C.c_longlong, C.c_int, _vp]),
     "qx_engine_config": (C.c_int, [_vp, C.c_int, _vp]),
+    "qx_set_engine": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
+    "qx_class_quartets": (C.c_int, [_vp, C.c_int, _ip]),
     "qx_compute_2e_int_noalloc": (
         C.c_int,
         [C.c_int, _dp, C.c_int, _ip, _ip, _ip, _dp, _dp, C.c_double, _vp, _vp],

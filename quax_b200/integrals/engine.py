@@ -188,7 +188,7 @@ class EriEngine:
             )
         return out
 
-    ENGINE_NAMES = ("sl", "warp", "coop", "wvrr", "wsplit", "dsplit")
+    ENGINE_NAMES = ("sl", "warp", "coop", "wvrr", "wsplit", "dsplit", "rys")
 
     def autotune(self, plain: bool = True, deriv: bool = True, stream=None) -> None:
         """Time every engine configuration per class on this molecule and keep the fastest."""
@@ -207,6 +207,39 @@ class EriEngine:
             _lib.check(lib.qx_engine_config(self.handle, c["cls"], C.c_void_p(cfg.ctypes.data)), "qx_engine_config")
             out["%d%d%d%d" % c["l"]] = (self.ENGINE_NAMES[cfg[0]], int(cfg[1]), self.ENGINE_NAMES[cfg[2]], int(cfg[3]))
         return out
+
+    def set_engine(self, cls: int, plain: str | None = None, plain_param: int = 0, deriv: str | None = None,
+                   deriv_param: int = 0) -> None:
+        """Force the engine of one class (names as in ENGINE_NAMES; None keeps the
+        current one).  plain_param: log2 lanes per quartet ("sl") or warps per
+        quartet ("warp": 1 or 4); deriv_param: warps per quartet ("warp")."""
+        pe = -1 if plain is None else self.ENGINE_NAMES.index(plain)
+        de = -1 if deriv is None else self.ENGINE_NAMES.index(deriv)
+        with torch.cuda.device(self.device):
+            _lib.check(_lib.load().qx_set_engine(self.handle, int(cls), pe, int(plain_param), de, int(deriv_param)),
+                       "qx_set_engine")
+
+    def class_quartets(self, cls: int) -> np.ndarray:
+        """(nq, 4) canonical shell indices of a class's quartets in list order (the
+        order of the unique layout)."""
+        nq = next(c["nq"] for c in self.class_info() if c["cls"] == cls)
+        out = np.zeros((max(nq, 1), 4), dtype=np.int32)
+        _lib.check(_lib.load().qx_class_quartets(self.handle, int(cls), _lib.iptr(out)), "qx_class_quartets")
+        return out[:nq]
+
+    def unique_blocks(self, out: torch.Tensor | None = None):
+        """{class id: (shells (nq, 4), blocks (nq, ncomp))} from the unique layout."""
+        u = self.eri_unique(out)
+        res = {}
+        base = 0
+        for c in self.class_info():
+            nq = c["nq"]
+            ncomp = int(np.prod([(l + 1) * (l + 2) // 2 for l in c["l"]]))
+            if nq:
+                blk = u[base:base + nq * ncomp].view(ncomp, nq).T
+                res[c["cls"]] = (self.class_quartets(c["cls"]), blk)
+            base += nq * ncomp
+        return res
 
     def grad_adjoint_jvp(self, D: torch.Tensor, v, cj: float = 1.0, ck: float = -0.5, stream=None) -> torch.Tensor:
         """Hessian-vector product of sum Gamma G (Gamma from D, fixed) along v (3N)."""
@@ -238,8 +271,9 @@ class EriEngine:
 
     # -- derivatives ----------------------------------------------------------
     def eri_deriv_core(self, order: int = 1, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
-        """Dense derivative tensor on the device, reference layout: (3N, n, n, n, n) for
-        order 1, (3N(3N+1)/2, n, n, n, n) for order 2 (nuclear pairs nu1 <= nu2)."""
+        """Dense derivative tensor on the device, reference layout (nderiv, n, n, n, n):
+        nderiv = 3N for order 1, 3N(3N+1)/2 for order 2 (nuclear pairs nu1 <= nu2), and
+        in general the combinations with repetition of the 3N coordinates (orders 1-4)."""
         n = self.nbf
         shape = (how_many_derivs(self.natom, int(order)), n, n, n, n)
         if out is None:

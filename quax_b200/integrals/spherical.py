@@ -29,29 +29,55 @@ from ..basis import Basis, cart_components
 from .engine import EriEngine
 
 
+def _solid_harmonic_monomials(l: int, m: int):
+    """{(a, b, c): coefficient} of the real solid harmonic S_lm as a polynomial in
+    x, y, z (Helgaker, Jorgensen & Olsen, Molecular Electronic-Structure Theory,
+    eqs. 6.4.47-6.4.50: the sum over t, u, v of binomial products, v running over
+    half-integers for m < 0), before normalisation."""
+    am = abs(m)
+    vm = 0.0 if m >= 0 else 0.5
+    out = {}
+    for t in range((l - am) // 2 + 1):
+        for u in range(t + 1):
+            v = vm
+            while v <= (am / 2.0 - vm) // 1 + vm + 1e-9:
+                c = ((-1) ** int(round(t + v - vm)) * 0.25 ** t * math.comb(l, t) * math.comb(l - t, am + t)
+                     * math.comb(t, u) * math.comb(am, int(round(2 * v))))
+                a = 2 * t + am - int(round(2 * (u + v)))
+                b = int(round(2 * (u + v)))
+                key = (a, b, l - 2 * t - am)
+                out[key] = out.get(key, 0.0) + c
+                v += 1.0
+    return out
+
+
+def _dfact(n: int) -> float:
+    r = 1.0
+    while n > 1:
+        r *= n
+        n -= 2
+    return r
+
+
 def cart2sph(l: int) -> np.ndarray:
-    """(2l+1, ncart(l)) coefficients of the real solid harmonics over the Libint-
-    normalised Cartesian components."""
+    """(2l+1, ncart(l)) coefficients of the real solid harmonics (m = -l..l) over
+    the Libint-normalised Cartesian components (every component carries the
+    normalisation of x^l), each spherical function scaled to unit norm with the
+    Cartesian angular overlaps <x^a y^b z^c | x^a' y^b' z^c'> =
+    (a+a'-1)!! (b+b'-1)!! (c+c'-1)!! / (2l-1)!!  (zero unless every sum is even)."""
     comps = cart_components(l)
     idx = {c: k for k, c in enumerate(comps)}
+    S = np.zeros((len(comps), len(comps)))
+    for i, p in enumerate(comps):
+        for j, q in enumerate(comps):
+            e = [p[k] + q[k] for k in range(3)]
+            if all(x % 2 == 0 for x in e):
+                S[i, j] = _dfact(e[0] - 1) * _dfact(e[1] - 1) * _dfact(e[2] - 1) / _dfact(2 * l - 1)
     M = np.zeros((2 * l + 1, len(comps)))
-    if l == 0:
-        M[0, 0] = 1.0
-    elif l == 1:
-        for m, c in enumerate(((0, 1, 0), (0, 0, 1), (1, 0, 0))):  # y, z, x
-            M[m, idx[c]] = 1.0
-    elif l == 2:
-        r3 = math.sqrt(3.0)
-        M[0, idx[(1, 1, 0)]] = r3                       # xy
-        M[1, idx[(0, 1, 1)]] = r3                       # yz
-        M[2, idx[(0, 0, 2)]] = 1.0                      # zz - (xx + yy) / 2
-        M[2, idx[(2, 0, 0)]] = -0.5
-        M[2, idx[(0, 2, 0)]] = -0.5
-        M[3, idx[(1, 0, 1)]] = r3                       # xz
-        M[4, idx[(2, 0, 0)]] = 0.5 * r3                 # (xx - yy) sqrt(3) / 2
-        M[4, idx[(0, 2, 0)]] = -0.5 * r3
-    else:
-        raise NotImplementedError("spherical functions for l <= 2")
+    for r, m in enumerate(range(-l, l + 1)):
+        for key, c in _solid_harmonic_monomials(l, m).items():
+            M[r, idx[key]] += c
+        M[r] /= math.sqrt(M[r] @ S @ M[r])
     return M
 
 

@@ -31,9 +31,9 @@ def test_build_info():
     from quax_b200.integrals import _lib
 
     lib = _lib.load()
-    assert lib.qx_max_l() == 2
-    assert lib.qx_max_deriv_order() == 2
-    assert lib.qx_num_classes() == 21
+    assert lib.qx_max_l() == 3  # f shells
+    assert lib.qx_max_deriv_order() == 4
+    assert lib.qx_num_classes() == 55  # canonical classes up to (ff|ff)
 
 
 def _init(lib, _lib, coords, exps, tol=1e-12, l=(0,), nprim=(1,), atom=(0,)):

@@ -147,16 +147,18 @@ def test_deriv_errors():
     b = small_synthetic(0)  # carries d shells
     eng = _engine(b, 1e-12)
     with pytest.raises(NotImplementedError):
-        eng.eri_deriv_core(order=3)
+        eng.eri_deriv_core(order=5)
     with pytest.raises(NotImplementedError):
-        eng.eri_deriv_core(order=2)
+        eng.eri_deriv_core(order=0)
     dv = np.zeros(3 * b.natom, dtype=int)
-    dv[0] = 2
+    dv[0] = 5
     with pytest.raises(NotImplementedError):
         eng.eri_deriv(dv)
-    dv[0] = 3
-    with pytest.raises(NotImplementedError):
+    dv[0] = -1
+    with pytest.raises(ValueError):
         eng.eri_deriv(dv)
+    with pytest.raises(NotImplementedError):
+        eng.eri_deriv(np.zeros(3 * b.natom, dtype=int))  # order 0
     with pytest.raises(ValueError):
         eng.eri_deriv(np.zeros(5, dtype=int))
 
@@ -205,9 +207,8 @@ def test_grad_adjoint_jvp(seed):
 
 
 def test_grad_adjoint_jvp_errors():
-    eng = _engine(small_synthetic(0), 1e-12)  # d shells: no order-2 programs in this build
+    eng = _engine(small_synthetic(0), 1e-12)
     D = torch.eye(eng.nbf, dtype=torch.float64).cuda()
-    with pytest.raises(NotImplementedError):
-        eng.grad_adjoint_jvp(D, np.zeros(3 * eng.natom))
+    assert np.abs(eng.grad_adjoint_jvp(D, np.zeros(3 * eng.natom)).cpu().numpy()).max() == 0.0
     with pytest.raises(ValueError):
         eng.grad_adjoint_jvp(D, np.zeros(5))
