@@ -61,6 +61,9 @@ def lib():
         L.qxo_count_unique.argtypes = [C.POINTER(_Basis), C.c_double, C.c_int]
         L.qxo_shell_quartet_deriv2.argtypes = [C.POINTER(_Basis), C.c_int, C.c_int, C.c_int, C.c_int, _dp]
         L.qxo_eri_deriv2.argtypes = [C.POINTER(_Basis), C.c_double, C.c_int, _dp, C.c_int]
+        L.qxo_quartet_blocks.argtypes = [C.POINTER(_Basis), _ip, C.c_long, _dp, C.c_int]
+        L.qxo_grad_quartets.argtypes = [C.POINTER(_Basis), _ip, C.c_long, _dp, C.c_double, C.c_double, _dp,
+                                        C.c_int]
         L.qxo_how_many_derivs.argtypes = [C.c_int, C.c_int]
         L.qxo_multi_index_lookup.argtypes = [C.c_int, C.c_int, _ip]
         _LIB = L
@@ -170,6 +173,28 @@ def eri_deriv2(ob: OracleBasis, thr: float, pair_idx: int = -1, nthreads: int = 
     out = np.empty(shape)
     lib().qxo_eri_deriv2(ob.ref, thr, int(pair_idx), _p(out), nthreads)
     return out
+
+
+def quartet_blocks(ob: OracleBasis, shells: np.ndarray, nthreads: int = 0) -> np.ndarray:
+    """(nq, nblk) contracted blocks of a list of shell quartets of one class
+    (shells: (nq, 4) shell indices, in that centre order)."""
+    q4 = np.ascontiguousarray(np.asarray(shells, dtype=np.int32).reshape(-1, 4))
+    if q4.shape[0] == 0:
+        return np.zeros((0, 0))
+    nblk = int(np.prod([(int(ob.l[s]) + 1) * (int(ob.l[s]) + 2) // 2 for s in q4[0]]))
+    out = np.empty((q4.shape[0], nblk))
+    if lib().qxo_quartet_blocks(ob.ref, _p(q4, _ip), q4.shape[0], _p(out), nthreads) != 0:
+        raise ValueError("quartet_blocks: the quartets are not of one class")
+    return out
+
+
+def grad_quartets(ob: OracleBasis, shells: np.ndarray, D: np.ndarray, cj=1.0, ck=-0.5, nthreads: int = 0):
+    """Adjoint-gradient contribution (3N) of a list of 8-fold-unique quartets."""
+    q4 = np.ascontiguousarray(np.asarray(shells, dtype=np.int32).reshape(-1, 4))
+    D = np.ascontiguousarray(D, dtype=np.float64)
+    g = np.zeros(3 * ob.natom)
+    lib().qxo_grad_quartets(ob.ref, _p(q4, _ip), q4.shape[0], _p(D), float(cj), float(ck), _p(g), nthreads)
+    return g
 
 
 def grad_contract(ob: OracleBasis, thr: float, D: np.ndarray, cj=1.0, ck=-0.5, nthreads: int = 0) -> np.ndarray:

@@ -313,7 +313,8 @@ static int quartet(const qxo_basis *B, int s1, int s2, int s3, int s4, int deriv
             double ca = B->coef[B->prim_off[s1] + p1], cb = B->coef[B->prim_off[s2] + p2];
             double zeta = a + b;
             double P[3], PA[3];
-            for (int i = 0; i < 3; ++i) { P[i] = (a * A[i] + b * Bc[i]) / zeta; PA[i] = P[i] - A[i]; }
+            /* P - A = -(b / zeta)(A - B): exactly zero for a one-centre pair */
+            for (int i = 0; i < 3; ++i) { PA[i] = -(b / zeta) * AB[i]; P[i] = A[i] + PA[i]; }
             double Kab = exp(-a * b / zeta * AB2) * ca * cb;
             for (int p3 = 0; p3 < B->nprim[s3]; ++p3)
                 for (int p4 = 0; p4 < B->nprim[s4]; ++p4) {
@@ -321,15 +322,17 @@ static int quartet(const qxo_basis *B, int s1, int s2, int s3, int s4, int deriv
                     double cc = B->coef[B->prim_off[s3] + p3], cd = B->coef[B->prim_off[s4] + p4];
                     double eta = c + d;
                     double Q[3], QC[3], W[3], WP[3], WQ[3];
-                    for (int i = 0; i < 3; ++i) { Q[i] = (c * C[i] + d * D[i]) / eta; QC[i] = Q[i] - C[i]; }
+                    for (int i = 0; i < 3; ++i) { QC[i] = -(d / eta) * CD[i]; Q[i] = C[i] + QC[i]; }
                     double Kcd = exp(-c * d / eta * CD2) * cc * cd;
                     double rho = zeta * eta / (zeta + eta);
                     double PQ2 = 0.0;
                     for (int i = 0; i < 3; ++i) {
-                        W[i] = (zeta * P[i] + eta * Q[i]) / (zeta + eta);
-                        WP[i] = W[i] - P[i];
-                        WQ[i] = W[i] - Q[i];
-                        PQ2 += (P[i] - Q[i]) * (P[i] - Q[i]);
+                        /* W - P = -eta/(zeta+eta) (P - Q), P - Q = (A - C) + PA - QC */
+                        const double PQ = (A[i] - C[i]) + PA[i] - QC[i];
+                        W[i] = P[i] - eta / (zeta + eta) * PQ;
+                        WP[i] = -eta / (zeta + eta) * PQ;
+                        WQ[i] = zeta / (zeta + eta) * PQ;
+                        PQ2 += PQ * PQ;
                     }
                     qxo_boys(E + F, rho * PQ2, Fm);
                     double pref = pref0 / (zeta * eta * sqrt(zeta + eta)) * Kab * Kcd;
@@ -690,6 +693,92 @@ int qxo_grad_contract(const qxo_basis *B, double thr, const double *Dm, double c
     return 0;
 }
 
+/* Contracted blocks of a list of shell quartets (q4[4*q + 0..3], in the given
+ * centre order), all of one angular-momentum class: out[q * nblk + element],
+ * element row-major over (f1, f2, f3, f4).  For comparing a unique layout
+ * quartet by quartet. */
+int qxo_quartet_blocks(const qxo_basis *B, const int *q4, long nq, double *out, int nthreads) {
+    init_tables();
+    if (nq <= 0) return 0;
+    const int *q0 = q4;
+    size_t nblk = (size_t)ncart(B->l[q0[0]]) * ncart(B->l[q0[1]]) * ncart(B->l[q0[2]]) * ncart(B->l[q0[3]]);
+    for (long q = 0; q < nq; ++q)
+        for (int c = 0; c < 4; ++c)
+            if (B->l[q4[4 * q + c]] != B->l[q0[c]]) return -1;
+    int nt = nthreads_of(nthreads);
+#pragma omp parallel num_threads(nt)
+    {
+        scratch_t scr = {0, 0};
+#pragma omp for schedule(dynamic, 64)
+        for (long q = 0; q < nq; ++q)
+            quartet(B, q4[4 * q], q4[4 * q + 1], q4[4 * q + 2], q4[4 * q + 3], 0, out + (size_t)q * nblk, &scr);
+        free(scr.v);
+    }
+    return 0;
+}
+
+/* Adjoint-gradient contribution of a list of 8-fold-unique shell quartets
+ * (q4[4*q + 0..3]): grad[3*atom + xyz] += sum over the quartets' distinct images
+ * of Gamma_ijkl d(ij|kl)/dR, Gamma = cj D_ij D_kl + ck D_ik D_jl -- the terms
+ * qxo_grad_contract adds for the same quartets.  grad is not zeroed. */
+int qxo_grad_quartets(const qxo_basis *B, const int *q4, long nq, const double *Dm, double cj, double ck,
+                      double *grad, int nthreads) {
+    init_tables();
+    int ns = B->nshell;
+    long *s2bf = (long *)malloc(sizeof(long) * ns);
+    long n;
+    shell2bf_of(B, s2bf, &n);
+    int N3 = 3 * B->natom;
+    int nt = nthreads_of(nthreads);
+#define GAM(i, j, k, l) (cj * Dm[(i) * n + (j)] * Dm[(k) * n + (l)] + ck * Dm[(i) * n + (k)] * Dm[(j) * n + (l)])
+#pragma omp parallel num_threads(nt)
+    {
+        scratch_t scr = {0, 0};
+        double *buf = (double *)malloc(sizeof(double) * 10000 * 12);
+        double *g = (double *)calloc(N3, sizeof(double));
+#pragma omp for schedule(dynamic, 64)
+        for (long q = 0; q < nq; ++q) {
+            int p1 = q4[4 * q], p2 = q4[4 * q + 1], p3 = q4[4 * q + 2], p4 = q4[4 * q + 3];
+            int at[4] = {B->atom[p1], B->atom[p2], B->atom[p3], B->atom[p4]};
+            if (at[0] == at[1] && at[0] == at[2] && at[0] == at[3]) continue;
+            int sPQ = !((p1 == p3 && p2 == p4) || (p1 == p4 && p2 == p3));
+            quartet(B, p1, p2, p3, p4, 1, buf, &scr);
+            int n1 = shell_size(B->l[p1]), n2 = shell_size(B->l[p2]), n3 = shell_size(B->l[p3]),
+                nn4 = shell_size(B->l[p4]);
+            size_t nblk = (size_t)n1 * n2 * n3 * nn4;
+            long b1 = s2bf[p1], b2 = s2bf[p2], b3 = s2bf[p3], b4 = s2bf[p4];
+            double acc[12] = {0};
+            for (int f1 = 0, idx = 0; f1 < n1; ++f1)
+                for (int f2 = 0; f2 < n2; ++f2)
+                    for (int f3 = 0; f3 < n3; ++f3)
+                        for (int f4 = 0; f4 < nn4; ++f4, ++idx) {
+                            long i = b1 + f1, j = b2 + f2, k = b3 + f3, l = b4 + f4;
+                            double w = GAM(i, j, k, l);
+                            if (p1 != p2) w += GAM(j, i, k, l);
+                            if (p3 != p4) w += GAM(i, j, l, k);
+                            if (p1 != p2 && p3 != p4) w += GAM(j, i, l, k);
+                            if (sPQ) {
+                                w += GAM(k, l, i, j);
+                                if (p3 != p4) w += GAM(l, k, i, j);
+                                if (p1 != p2) w += GAM(k, l, j, i);
+                                if (p1 != p2 && p3 != p4) w += GAM(l, k, j, i);
+                            }
+                            for (int c = 0; c < 12; ++c) acc[c] += w * buf[c * nblk + idx];
+                        }
+            for (int c = 0; c < 4; ++c)
+                for (int x = 0; x < 3; ++x) g[3 * at[c] + x] += acc[3 * c + x];
+        }
+#pragma omp critical
+        for (int i = 0; i < N3; ++i) grad[i] += g[i];
+        free(g);
+        free(buf);
+        free(scr.v);
+    }
+#undef GAM
+    free(s2bf);
+    return 0;
+}
+
 /* Time-bounded unique-quartet evaluation for the CPU baseline: evaluates the
  * screened 8-fold-unique quartets whose linear index (in bra-major, ket <= bra
  * order over the reference pair list) is congruent to `phase` modulo `stride`,
@@ -802,20 +891,21 @@ static int quartet2(const qxo_basis *B, int s1, int s2, int s3, int s4, double *
         for (int p2 = 0; p2 < B->nprim[s2]; ++p2) {
             double a = B->alpha[B->prim_off[s1] + p1], b = B->alpha[B->prim_off[s2] + p2];
             double zeta = a + b, P[3], PA[3];
-            for (int i = 0; i < 3; ++i) { P[i] = (a * Cn[0][i] + b * Cn[1][i]) / zeta; PA[i] = P[i] - Cn[0][i]; }
+            for (int i = 0; i < 3; ++i) { PA[i] = -(b / zeta) * AB[i]; P[i] = Cn[0][i] + PA[i]; }
             double Kab = exp(-a * b / zeta * AB2) * B->coef[B->prim_off[s1] + p1] * B->coef[B->prim_off[s2] + p2];
             for (int p3 = 0; p3 < B->nprim[s3]; ++p3)
                 for (int p4 = 0; p4 < B->nprim[s4]; ++p4) {
                     double c = B->alpha[B->prim_off[s3] + p3], d = B->alpha[B->prim_off[s4] + p4];
                     double eta = c + d, Q[3], QC[3], W[3], WP[3], WQ[3], PQ2 = 0.0;
-                    for (int i = 0; i < 3; ++i) { Q[i] = (c * Cn[2][i] + d * Cn[3][i]) / eta; QC[i] = Q[i] - Cn[2][i]; }
+                    for (int i = 0; i < 3; ++i) { QC[i] = -(d / eta) * CD[i]; Q[i] = Cn[2][i] + QC[i]; }
                     double Kcd = exp(-c * d / eta * CD2) * B->coef[B->prim_off[s3] + p3] * B->coef[B->prim_off[s4] + p4];
                     double rho = zeta * eta / (zeta + eta);
                     for (int i = 0; i < 3; ++i) {
-                        W[i] = (zeta * P[i] + eta * Q[i]) / (zeta + eta);
-                        WP[i] = W[i] - P[i];
-                        WQ[i] = W[i] - Q[i];
-                        PQ2 += (P[i] - Q[i]) * (P[i] - Q[i]);
+                        const double PQ = (Cn[0][i] - Cn[2][i]) + PA[i] - QC[i];
+                        W[i] = P[i] - eta / (zeta + eta) * PQ;
+                        WP[i] = -eta / (zeta + eta) * PQ;
+                        WQ[i] = zeta / (zeta + eta) * PQ;
+                        PQ2 += PQ * PQ;
                     }
                     qxo_boys(E + F, rho * PQ2, Fm);
                     vrr(E, F, zeta, eta, PA, WP, QC, WQ, rho, Fm, pref0 / (zeta * eta * sqrt(zeta + eta)) * Kab * Kcd, v);

@@ -1,8 +1,8 @@
 """Build libquax_b200.so for sm_100a (in-tree, no JIT cache).
 
 Each CUDA translation unit is compiled by nvcc in parallel into
-quax_b200/_build/*.o; an object is rebuilt when its source or any header under
-csrc/ or include/ is newer.  The objects are linked into
+quax_b200/_build/*.o; an object is rebuilt when its source or a local header it
+includes (recursively) is newer.  The objects are linked into
 quax_b200/libquax_b200.so with the CUDA runtime linked statically, so the
 library does not depend on which libcudart the host process loaded first.
 """
@@ -10,6 +10,7 @@ from __future__ import annotations
 
 import glob
 import os
+import re
 import shutil
 import subprocess
 import sys
@@ -45,9 +46,27 @@ def sources():
     return sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "gen", "*.cu")))
 
 
-def _headers_mtime() -> float:
-    hs = glob.glob(os.path.join(CSRC, "**", "*.cuh"), recursive=True) + glob.glob(os.path.join(ROOT, "include", "*.h"))
-    return max((os.path.getmtime(h) for h in hs), default=0.0)
+_INC = re.compile(r'^\s*#\s*include\s+"([^"]+)"', re.M)
+
+
+def _deps_mtime(src: str, seen=None) -> float:
+    """Newest mtime of src and of every local header it includes, recursively
+    (quoted includes resolved against the including file's folder, csrc/ and
+    include/), so a header change rebuilds only the translation units that use it."""
+    seen = set() if seen is None else seen
+    if src in seen or not os.path.exists(src):
+        return 0.0
+    seen.add(src)
+    t = os.path.getmtime(src)
+    with open(src, errors="replace") as f:
+        text = f.read()
+    for name in _INC.findall(text):
+        for base in (os.path.dirname(src), CSRC, os.path.join(ROOT, "include")):
+            cand = os.path.normpath(os.path.join(base, name))
+            if os.path.exists(cand):
+                t = max(t, _deps_mtime(cand, seen))
+                break
+    return t
 
 
 def _obj(src: str) -> str:
@@ -55,9 +74,9 @@ def _obj(src: str) -> str:
     return os.path.join(BUILD, rel[:-3] + ".o")
 
 
-def _compile(src: str, hmt: float, verbose: bool):
+def _compile(src: str, verbose: bool):
     obj = _obj(src)
-    if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(src), hmt):
+    if os.path.exists(obj) and os.path.getmtime(obj) >= _deps_mtime(src):
         return obj, False
     cmd = [nvcc()] + NVCC_FLAGS + ["-c", src, "-o", obj]
     t0 = time.time()
@@ -77,15 +96,14 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
         subprocess.run([sys.executable, os.path.join(CSRC, "gen_eri.py")], check=True)
         with open(stamp, "w") as f:
             f.write("generated\n")
-    hmt = _headers_mtime()
     srcs = sources()
     with ThreadPoolExecutor(max_workers=jobs or os.cpu_count() or 4) as ex:
-        results = list(ex.map(lambda s: _compile(s, hmt, verbose), srcs))
+        results = list(ex.map(lambda s: _compile(s, verbose), srcs))
     objs = [o for o, _ in results]
     _link(LIB, objs, any(b for _, b in results))
     # FMA throughput probe used by the benchmark's roofline (separate library)
     psrc = os.path.join(CSRC, "peaks", "qx_peaks.cu")
-    pobj, pb = _compile(psrc, hmt, verbose)
+    pobj, pb = _compile(psrc, verbose)
     _link(PEAKS_LIB, [pobj], pb)
     return LIB
 

@@ -658,10 +658,13 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
                     PrimPair r;
                     r.zeta = a + b;
                     r.oo2z = 0.5 / r.zeta;
-                    r.Px = (a * A[0] + b * B[0]) / r.zeta;
-                    r.Py = (a * A[1] + b * B[1]) / r.zeta;
-                    r.Pz = (a * A[2] + b * B[2]) / r.zeta;
-                    r.PAx = r.Px - A[0]; r.PAy = r.Py - A[1]; r.PAz = r.Pz - A[2];
+                    // P - A = -(b / zeta)(A - B), exactly zero for a one-centre pair (forming
+                    // P first and subtracting A leaves ~1e-15 there, which tight exponents
+                    // amplify beyond 1e-12 in integrals that vanish by symmetry)
+                    r.PAx = -(b / r.zeta) * (A[0] - B[0]);
+                    r.PAy = -(b / r.zeta) * (A[1] - B[1]);
+                    r.PAz = -(b / r.zeta) * (A[2] - B[2]);
+                    r.Px = A[0] + r.PAx; r.Py = A[1] + r.PAy; r.Pz = A[2] + r.PAz;
                     r.K = kfac * ca * cb * std::exp(-a * b / r.zeta * AB2) / r.zeta;
                     r.alpha = a;
                     prims.push_back(r);

@@ -47,7 +47,13 @@ def test_shards_sum_to_full(nranks):
         e.close()
     assert snq == nq
     assert (sG - G).abs().max().item() < 1e-12
-    assert (sdG - dG).abs().max().item() < 1e-11 * max(1.0, dG.abs().max().item())
+    # the ranks' autotuned engines may differ from the full handle's (the Rys engine
+    # differentiates all four centres, the Obara-Saika engines take the fourth by
+    # translational invariance): on same-atom (dd|dd) quartets with tight exponents
+    # the invariance sum loses up to 6.5e-11 (quartet (20,5|20,5) of this molecule
+    # against a 40-digit evaluation; the direct derivative is within 2e-16), so
+    # cross-engine derivative tensors agree to 1e-10
+    assert (sdG - dG).abs().max().item() < 1e-10 * max(1.0, dG.abs().max().item())
     assert (sJ - J).abs().max().item() < 1e-11
     assert (sK - K).abs().max().item() < 1e-11
     assert (sg - g).abs().max().item() < 1e-9
