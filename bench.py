@@ -12,9 +12,12 @@ FP64 through the library's device path, with inputs resident in HBM.
   e2e     the same through the reference-facing C ABI with host buffers:
           qx_initialize (shells H2D) -> qx_compute_2e_int into pinned host memory
           (dense n^4 D2H, the reference's return convention) -> qx_finalize
-  extras  the HF-style geometric gradient sum Gamma dG of the same molecule by the
-          adjoint kernel and by the plain path (materialise the (3N,n^4) tensor,
-          then contract), seconds per evaluation
+  parity  the timed output against the CPU oracle, every quartet
+  gradient_headline
+          seconds per evaluation of sum Gamma dG/dR by the adjoint kernel and by
+          the plain derivative-tensor path (derivative integrals materialised tile
+          by tile as (3N, tile) tensors, then contracted): 10 and 30 atoms in full,
+          the 60-atom workload with f shells through a cost-balanced 1/64 shard
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 Under torchrun (N>1) each rank runs its own replica; the max over ranks is used.
@@ -38,6 +41,12 @@ if ROOT not in sys.path:
 METRIC = "HF geom-gradient s/eval (adjoint vs plain ERI-deriv) at 1e-8 Eh/bohr; quartets/s"
 WORKLOAD = "eri10"
 THR = 1e-12
+# DRAM traffic of a class's dominant kernel from an ncu capture of this workload
+# (dram__bytes_read.sum + dram__bytes_write.sum), with the capture it comes from
+TRAFFIC_FROM_PROFILE = {
+    (2, 2, 2, 1): {"bytes": 29.21e6, "source": "ncu capture in profiles/k_gvrr_p19_eri10.md (split VRR kernel "
+                                               "of the class, one launch)"},
+}
 
 
 def workload_desc(b, extra=None):
@@ -142,6 +151,34 @@ def cpu_baseline_eri(basis, target_s=12.0):
                       f"Schwarz pass excluded); C/OpenMP oracle, FP64"}
 
 
+def parity_vs_oracle(eng, b, out):
+    """The timed output against the oracle: every screened unique quartet's block
+    (class by class, list order) compared with the oracle's block of the same
+    canonical shell quartet (oracle on all host threads)."""
+    import numpy as np
+    import torch
+
+    from oracle import api
+
+    ob = api.OracleBasis(b)
+    base, err, err_scaled, nq_tot = 0, 0.0, 0.0, 0
+    t0 = time.perf_counter()
+    for c in eng.class_info():
+        nq = c["nq"]
+        ncomp = int(np.prod([(l + 1) * (l + 2) // 2 for l in c["l"]]))
+        if nq:
+            ref = torch.from_numpy(api.quartet_blocks(ob, eng.class_quartets(c["cls"]))).cuda()
+            d = (out[base:base + nq * ncomp].view(ncomp, nq).T - ref).abs()
+            err = max(err, float(d.max()))
+            err_scaled = max(err_scaled, float((d.amax(dim=1) / ref.abs().amax(dim=1).clamp(min=1.0)).max()))
+            nq_tot += nq
+        base += nq * ncomp
+    return {"max_abs_err": err, "max_err_over_block_scale": err_scaled, "quartets_checked": nq_tot,
+            "oracle": "C/OpenMP Obara-Saika/Head-Gordon-Pople restatement (oracle/eri_oracle.c), FP64",
+            "block_scale": "max(1, largest |integral| of the quartet's block)",
+            "oracle_s": time.perf_counter() - t0}
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -240,10 +277,12 @@ def run_ours(args):
         "unit": "TFLOP/s",
         "frac": achieved / peak if peak > 0 else None,
         "peak_source": "measured FP64 FMA probe (libqx_peaks.so), not in MEASURED_PEAKS.json",
-        # DRAM bytes per launch of the dominant kernel from one ncu capture
-        # (profiles/k_gvrr_p19_eri10.md); null when another class dominates
-        "traffic": 29.21e6 if tuple(dom["l"]) == (2, 2, 2, 1) else None,
-        "traffic_unit": "bytes per launch (VRR split kernel of the class, ncu)",
+        # DRAM bytes per launch of the dominant kernel: copied from one ncu capture
+        # of the same workload (not measured by this run), null for other classes
+        "traffic": TRAFFIC_FROM_PROFILE.get(tuple(dom["l"]), {}).get("bytes"),
+        "traffic_unit": "bytes per launch",
+        "traffic_source": TRAFFIC_FROM_PROFILE.get(tuple(dom["l"]), {}).get("source",
+                                                                           "no ncu capture of this class's kernel"),
         "step_achieved_tflops": total_flops / (ms_per_step * 1e-3) / 1e12,
         "dominant_share_of_serial_sum": dom_ms / sum(p[0] for p in per),
     }
@@ -301,12 +340,12 @@ def run_ours(args):
                  "path": "Cartesian unique kernels + per-class solid-harmonic transforms (cuBLAS DGEMM)"}
     sph.close()
 
-    grad = None
+    grad = batched = None
     if not args.no_grad:
-        grad = gradient_extras(eng, b, n, args.warmup)
-        grad["workload_30_atoms"] = gradient_30_atoms()
-        grad["batched_rhf"] = batched_extras(args.batch)
+        grad = gradient_headline(eng, b, oracle_check=rank == 0)
+        batched = batched_extras(args.batch)
 
+    parity = parity_vs_oracle(eng, b, out) if rank == 0 else None
     cpu = cpu_baseline_eri(b) if rank == 0 else None
     if rank == 0:
         line = {
@@ -330,7 +369,9 @@ def run_ours(args):
             "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clocks,
-            "gradient": grad,
+            "parity": parity,
+            "gradient_headline": grad,
+            "batched_rhf": batched,
             "spherical": spherical,
         }
         print(json.dumps(line), flush=True)
@@ -339,102 +380,188 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def gradient_extras(eng, b, n, warmup):
-    """Adjoint vs plain gradient sum Gamma dG (HF Gamma from a random density)."""
+def _density(n, seed=0):
+    """D = C C^T, C an n x n/4 matrix of iid N(0, 1/n) entries (the 30-atom
+    workload's definition of Gamma's density)."""
     import numpy as np
     import torch
 
-    rng = np.random.default_rng(0)
-    C = rng.normal(0.0, 1.0 / np.sqrt(n), size=(n, n // 4))
-    D = torch.from_numpy(C @ C.T).cuda()
-    for _ in range(max(1, warmup)):
-        g = eng.grad_adjoint(D)
+    rng = np.random.default_rng(seed)
+    C = rng.normal(0.0, 1.0 / np.sqrt(n), size=(n, max(1, n // 4)))
+    return torch.from_numpy(C @ C.T).cuda()
+
+
+def _time_ms(fn, reps=1, warm=True):
+    """Device time of fn() (CUDA events on the current stream; one warm-up call
+    unless warm is False, for long calls whose kernels already ran)."""
+    import torch
+
+    if warm:
+        fn()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    reps = 3
     e0.record()
     for _ in range(reps):
-        g = eng.grad_adjoint(D)
+        fn()
     e1.record()
     torch.cuda.synchronize()
-    adj_s = e0.elapsed_time(e1) / reps * 1e-3
-    out = {"adjoint_s": adj_s, "plain_s": None, "max_abs_diff_Eh_per_bohr": None,
-           "gamma": "cj D_ij D_kl + ck D_ik D_jl, cj=1, ck=-1/2, D = C C^T, C n x n/4 N(0,1/n)"}
-    need = 8 * (3 * b.natom * n**4 + n**4)
-    free, _ = torch.cuda.mem_get_info()
-    if need < 0.9 * free:
-        dG = torch.empty((3 * b.natom, n, n, n, n), dtype=torch.float64, device="cuda")
-        Gam = torch.einsum("ij,kl->ijkl", D, D) - 0.5 * torch.einsum("ik,jl->ijkl", D, D)
-        eng.eri_deriv_core(out=dG)
-        torch.cuda.synchronize()
-        e0.record()
-        eng.eri_deriv_core(out=dG)
-        gv = Gam.view(-1)
-        gp = torch.stack([torch.dot(dG[x].view(-1), gv) for x in range(3 * b.natom)])
-        e1.record()
-        torch.cuda.synchronize()
-        out["plain_s"] = e0.elapsed_time(e1) * 1e-3
-        out["max_abs_diff_Eh_per_bohr"] = float((gp - g).abs().max())
-        out["adjoint_speedup_vs_plain"] = out["plain_s"] / adj_s
-        del dG, Gam
-        torch.cuda.empty_cache()
-    else:
-        out["plain_s"] = f"skipped: needs {need / 1e9:.0f} GB"
-    return out
+    return e0.elapsed_time(e1) / reps
 
 
-def gradient_30_atoms():
-    """The 30-atom adjoint-gradient workload: adjoint s/eval, and the plain path
-    timed on one of its 3N derivative slices (the full (3N, n^4) tensor is
-    ~12 TB), so plain_s is an estimate: 3N x one slice's compute + contraction."""
+def _tile_engines(eng, D, shard=8, view=(0, 1)):
+    """Per class, the fastest derivative engine among those the plain path can also
+    use (warp kernels with 1 or 4 warps per quartet, Rys), timed in adjoint mode on
+    a 1/shard cost-balanced shard of the lists, so the adjoint and the plain path
+    below run the same derivative arithmetic."""
+    import torch
+
+    g = torch.zeros(3 * eng.natom, dtype=torch.float64, device="cuda")
+    cfg = eng.engine_config()
+    if view == (0, 1):
+        eng.set_shard(0, shard)  # an unsharded handle is timed on a shard
+    for c in eng.class_info():
+        if not c["nq"] or cfg["%d%d%d%d" % c["l"]][2] in ("warp", "rys"):
+            continue  # the autotuned engine has the tile epilogue already
+        best = None
+        for name, p in (("warp", 1), ("warp", 4), ("rys", 0)):
+            try:
+                eng.set_engine(c["cls"], deriv=name, deriv_param=p)
+            except NotImplementedError:
+                continue
+            ms = _time_ms(lambda: eng.grad_adjoint_class(c["cls"], D, g))
+            if best is None or ms < best[0]:
+                best = (ms, name, p)
+        eng.set_engine(c["cls"], deriv=best[1], deriv_param=best[2])
+    if view == (0, 1):
+        eng.set_shard(0, 1)
+
+
+def _autotune_on_shard(eng, shard, plain=False):
+    """Engines per class chosen by the autotuner on a 1/shard cost-balanced shard
+    of the lists (the choices persist when the full lists are restored)."""
+    eng.set_shard(0, shard)
+    eng.autotune(plain=plain, deriv=True)
+    eng.set_shard(0, 1)
+
+
+def _adjoint_vs_plain(eng, D, reps=1, warm=True, unique=True, view=(0, 1)):
+    """Adjoint gradient vs the plain derivative-tensor path on one handle: the
+    adjoint with the autotuned engines, then both paths with the same per-class
+    engines (the plain path materialises every derivative integral -- each image
+    of the reference's (3N, n^4) tensor, tile by tile -- and contracts the tiles
+    with Gamma; each derivative quartet is evaluated once)."""
+    r = {"adjoint_autotuned_s": _time_ms(lambda: eng.grad_adjoint(D), reps, warm) * 1e-3}
+    _tile_engines(eng, D, view=view)
+    ga = eng.grad_adjoint(D)  # also warms the chosen engines
+    r["adjoint_s"] = _time_ms(lambda: eng.grad_adjoint(D), reps, False) * 1e-3
+    gp = eng.grad_plain(D, images=True)
+    r["plain_s"] = _time_ms(lambda: eng.grad_plain(D, images=True), reps, False) * 1e-3
+    if unique:
+        r["plain_unique_elements_s"] = _time_ms(lambda: eng.grad_plain(D, images=False), reps, False) * 1e-3
+    r["max_abs_diff_adjoint_vs_plain_Eh_per_bohr"] = float((ga - gp).abs().max())
+    r["adjoint_speedup_vs_plain"] = r["plain_s"] / r["adjoint_s"]
+    r["tile_engines"] = {k: v[2] for k, v in eng.engine_config().items()}
+    return r, ga
+
+
+def _hessian_column(eng, D, warm=True):
+    import torch
+
+    e0 = torch.zeros(3 * eng.natom, dtype=torch.float64)
+    e0[0] = 1.0
+    return _time_ms(lambda: eng.grad_adjoint_jvp(D, e0), 1, warm) * 1e-3
+
+
+def gradient_headline(eng10, b10, oracle_check=True):
+    """The north-star quantity: s per evaluation of the HF-type gradient
+    sum Gamma_ijkl d(ij|kl)/dR (Gamma = D_ij D_kl - 1/2 D_ik D_jl), adjoint kernel
+    vs the plain FP64 derivative-tensor path, on the 10- and 30-atom workloads in
+    full and on the 60-atom workload with f shells through a cost-balanced shard."""
     import numpy as np
     import torch
 
     from quax_b200.basis import config_spec, synthetic_molecule
     from quax_b200.integrals.engine import EriEngine
 
-    mol, b = synthetic_molecule(config_spec("grad30"), 0)
-    eng = EriEngine(b, THR)
-    n = eng.nbf
-    rng = np.random.default_rng(0)
-    C = rng.normal(0.0, 1.0 / np.sqrt(n), size=(n, n // 4))
-    D = torch.from_numpy(C @ C.T).cuda()
-    eng.grad_adjoint(D)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    g = eng.grad_adjoint(D)
-    e1.record()
-    torch.cuda.synchronize()
-    adj = e0.elapsed_time(e1) * 1e-3
-    out = {"natom": b.natom, "nbf": n, "unique_quartets": eng.unique_quartets(), "adjoint_s": adj,
-           "plain_s_estimate": None}
-    free, _ = torch.cuda.mem_get_info()
-    if 8 * n**4 * 1.15 < free:
-        # plain path, one nuclear index: the n^4 slice, then sum Gamma dG with
-        # Gamma = D_ij D_kl - 1/2 D_ik D_jl contracted row block by row block
-        nu = 0
-        dv = np.zeros(3 * b.natom, dtype=np.int64)
-        dv[nu] = 1
-        sl = torch.empty((n, n, n, n), dtype=torch.float64, device="cuda")
-        e0.record()
-        eng.eri_deriv(dv, out=sl)
-        acc = torch.zeros((), dtype=torch.float64, device="cuda")
-        for i0 in range(0, n, 16):
-            blk = sl[i0:i0 + 16]  # (bi, n, n, n)
-            acc += torch.einsum("ajkl,aj,kl->", blk, D[i0:i0 + 16], D)
-            acc -= 0.5 * torch.einsum("ajkl,ak,jl->", blk, D[i0:i0 + 16], D)
-        e1.record()
-        torch.cuda.synchronize()
-        one = e0.elapsed_time(e1) * 1e-3
-        out["plain_s_estimate"] = one * 3 * b.natom
-        out["plain_slice_s"] = one
-        out["slice_check_abs_diff"] = abs(float(acc) - float(g[nu]))
-        out["adjoint_speedup_vs_plain_estimate"] = out["plain_s_estimate"] / adj
-        del sl
-        torch.cuda.empty_cache()
-    eng.close()
+    out = {"gamma": "D_ij D_kl - 1/2 D_ik D_jl, D = C C^T, C n x n/4 iid N(0,1/n), seed 0",
+           "plain_path": "first-derivative integrals of tiles of unique quartets materialised as (3N, tile) "
+                         "tensors holding every image of each integral (the reference tensor's elements), "
+                         "then one GEMV per tile with Gamma; each derivative quartet evaluated once"}
+    # 10 atoms: error against the oracle over a contiguous eighth of every class
+    D10 = _density(eng10.nbf)
+    w10, _ = _adjoint_vs_plain(eng10, D10, reps=3)
+    w10["hessian_column_jvp_s"] = _hessian_column(eng10, D10)
+    if oracle_check:
+        from oracle import api
+
+        ob = api.OracleBasis(b10)
+        eng10.set_shard(0, 8)
+        err, gmax = 0.0, 0.0
+        g = torch.zeros(3 * b10.natom, dtype=torch.float64, device="cuda")
+        for c in eng10.class_info():
+            if not c["nq"]:
+                continue
+            g.zero_()
+            eng10.grad_adjoint_class(c["cls"], D10, g)
+            ref = api.grad_quartets(ob, eng10.class_quartets(c["cls"]), D10.cpu().numpy(), 1.0, -0.5)
+            err = max(err, float(np.abs(g.cpu().numpy() - ref).max()))
+            gmax = max(gmax, float(np.abs(ref).max()))
+        eng10.set_shard(0, 1)
+        w10["max_abs_err_vs_oracle_Eh_per_bohr"] = err
+        w10["oracle_sample"] = "per class, the contiguous eighth of its quartet list with the most primitives"
+    out["workload_10_atoms"] = w10
+    # 30 atoms (l <= 2), in full
+    _, b30 = synthetic_molecule(config_spec("grad30"), 0)
+    t0 = time.perf_counter()
+    e30 = EriEngine(b30, THR)
+    init30 = time.perf_counter() - t0
+    D30 = _density(e30.nbf)
+    _autotune_on_shard(e30, 8)
+    w30, g64 = _adjoint_vs_plain(e30, D30, warm=True)
+    w30.update({"natom": b30.natom, "nbf": e30.nbf, "unique_quartets": e30.unique_quartets(), "init_s": init30,
+                "engines": "derivative engines autotuned on a 1/8 cost-balanced shard of the lists"})
+    # mixed precision over the whole molecule: FP32 recurrences below a Schwarz
+    # bound of 1e-6 (reorders the lists, so measured unsharded), error vs FP64
+    e30.set_precision(1e-6)
+    g32 = e30.grad_adjoint(D30)
+    w30["mixed_precision"] = {"bound": 1e-6, "adjoint_s": _time_ms(lambda: e30.grad_adjoint(D30), 1, False) * 1e-3,
+                              "max_abs_dgrad_vs_fp64_Eh_per_bohr": float((g32 - g64).abs().max())}
+    e30.close()
+    out["workload_30_atoms"] = w30
+    out["workload_60_atoms_f"] = gradient_60_atoms()
     return out
+
+
+def gradient_60_atoms(S=128):
+    """The 60-atom workload with f shells (K 1-3, exponents 0.2-5 on the heavy
+    atoms): every timing on rank S/2 of an S-way cost-balanced shard (each class
+    keeps a contiguous range of its quartets of about 1/S of its primitive work),
+    scaled by S to an s/eval estimate -- the full evaluation runs minutes."""
+    import torch
+
+    from quax_b200.basis import config_spec, synthetic_molecule
+    from quax_b200.integrals.engine import EriEngine
+
+    _, b = synthetic_molecule(config_spec("mixed60"), 0)
+    t0 = time.perf_counter()
+    eng = EriEngine(b, THR)
+    init = time.perf_counter() - t0
+    info = eng.class_info()
+    r = {"natom": b.natom, "nbf_cartesian": eng.nbf, "unique_quartets": eng.unique_quartets(),
+         "f_quartets": sum(c["nq"] for c in info if max(c["l"]) == 3),
+         "primitive_quartets": sum(c["prims"] for c in info), "init_s": init,
+         "sample": f"rank {S // 2} of {S} cost-balanced shards; times x {S}"}
+    eng.set_shard(S // 2, S)
+    eng.autotune(plain=True, deriv=True)
+    D = _density(eng.nbf)
+    r["jk_s_estimate"] = _time_ms(lambda: eng.jk(D)) * 1e-3 * S
+    a, _ = _adjoint_vs_plain(eng, D, warm=False, unique=False, view=(S // 2, S))
+    for k in ("adjoint_autotuned_s", "adjoint_s", "plain_s"):
+        r[k.replace("_s", "_s_estimate")] = a[k] * S
+    r["adjoint_speedup_vs_plain"] = a["adjoint_speedup_vs_plain"]
+    r["max_abs_diff_adjoint_vs_plain_Eh_per_bohr (shard)"] = a["max_abs_diff_adjoint_vs_plain_Eh_per_bohr"]
+    eng.close()
+    return r
 
 
 def batched_extras(count: int, iterations: int = 20):
@@ -473,8 +600,8 @@ def batched_extras(count: int, iterations: int = 20):
     br.close()
     return {"molecules": count, "natom": mol0.natom, "nbf": b0.nbf(), "unique_quartets_per_jk": nq,
             "scf_iterations": iterations, "setup_s": t1 - t0, "scf_s": t2 - t1,
-            "jk_graph_ms_per_iteration": t_jk / iterations * 1e3, "jk_eager_ms": eager_ms,
-            "jk_quartets_per_s": nq / (t_jk / iterations), "gradients_s": t3 - t2,
+            "jk_graph_ms_per_iteration (incremental, density-screened builds)": t_jk / iterations * 1e3,
+            "full_jk_eager_ms": eager_ms, "full_jk_quartets_per_s": nq / (eager_ms * 1e-3), "gradients_s": t3 - t2,
             "energy_spread_Eh": float(max(E) - min(E)),
             "max_abs_gradient": float(max(abs(g).max() for g in G))}
 

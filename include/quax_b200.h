@@ -237,6 +237,24 @@ int qx_set_engine(qx_handle *h, int cls, int plain, int pparam, int deriv, int d
  * unique layout of qx_eri_unique back to shell quartets. */
 int qx_class_quartets(const qx_handle *h, int cls, int *shells);
 
+/* The plain (materialise-then-contract) derivative path, tile by tile, no
+ * counterpart as an entry point in the reference, whose gradient contracts the
+ * dense (3N, n^4) tensor of eri_deriv_core (libint_interface.cc:2582-2779) with
+ * Gamma under jacfwd (quax/methods/hartree_fock.py:79-80):
+ * qx_deriv_tile writes the first-derivative integrals of quartets [q0, q1) of a
+ * class (its unique-layout order) into B, a (3N, E) row-major device buffer the
+ * caller zeroes: row = nuclear index 3*atom + xyz, column = (q - q0) * ncomp +
+ * component (images = 0), or that index * 8 + image for each distinct image of
+ * the integral -- (ij|kl), (ji|kl), (ij|lk), (ji|lk), (kl|ij), (lk|ij), (kl|ji),
+ * (lk|ji) -- which are the reference tensor's elements (images = 1).
+ * qx_gamma_tile writes Gamma (cj D_ij D_kl + ck D_ik D_jl) for the same columns
+ * (summed over the distinct images when images = 0), so B @ gam summed over the
+ * tiles is the adjoint gradient.  Device pointers; asynchronous on `stream`. */
+int qx_deriv_tile(qx_handle *h, int cls, long long q0, long long q1, int images, double *B, long long E,
+                  void *stream);
+int qx_gamma_tile(qx_handle *h, int cls, long long q0, long long q1, int images, const double *D, double cj,
+                  double ck, double *gam, void *stream);
+
 /* Size of the fixed device array qx_compute_2e_int_noalloc works in. */
 #define QX_NOALLOC_SCRATCH_BYTES (16u << 20)
 

@@ -78,7 +78,12 @@ def _compile(src: str, verbose: bool):
     obj = _obj(src)
     if os.path.exists(obj) and os.path.getmtime(obj) >= _deps_mtime(src):
         return obj, False
-    cmd = [nvcc()] + NVCC_FLAGS + ["-c", src, "-o", obj]
+    flags = NVCC_FLAGS
+    if os.path.basename(src).startswith("k_rys_"):
+        # the 55 Rys-engine units carry ~7 kernels each; their line tables would
+        # more than double the library, so they are built without -lineinfo
+        flags = [f for f in NVCC_FLAGS if f != "-lineinfo"]
+    cmd = [nvcc()] + flags + ["-c", src, "-o", obj]
     t0 = time.time()
     r = subprocess.run(cmd, capture_output=True, text=True)
     if verbose:

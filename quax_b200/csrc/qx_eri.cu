@@ -1780,6 +1780,103 @@ extern "C" int qx_engine_config(const qx_handle* h, int cls, int* cfg) {
     return QX_OK;
 }
 
+// ------------------------------------------------- derivative tiles (plain path) --
+// Gamma of a tile of one class's unique quartets, in the layout of the derivative
+// tiles: per element (quartet-local qi, component o) the sum of Gamma over the
+// integral's distinct images (images = 0), or Gamma of each image in its slot of 8
+// (images = 1; absent images 0).  Gamma_ijkl = cj D_ij D_kl + ck D_ik D_jl.
+__global__ void __launch_bounds__(128) k_gamma_tile(const int2* __restrict__ quartets, long long nq,
+                                                    const PairInfo* __restrict__ pairs, int nb, int nc, int nd,
+                                                    int nout, const double* __restrict__ D, long long n, double cj,
+                                                    double ck, int images, double* __restrict__ gam) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nq * nout) return;
+    const long long qi = t / nout;
+    const int o = (int)(t - qi * nout);
+    const int2 pq = quartets[qi];
+    const PairInfo P = pairs[pq.x], Q = pairs[pq.y];
+    const int id = o % nd, ic = (o / nd) % nc, ib = (o / (nd * nc)) % nb, ia = o / (nd * nc * nb);
+    const long long i = P.bf1 + ia, j = P.bf2 + ib, k = Q.bf1 + ic, l = Q.bf2 + id;
+    const bool s12 = P.s1 != P.s2, s34 = Q.s1 != Q.s2, sPQ = pq.x != pq.y;
+    auto G = [&](long long p, long long q, long long r, long long s) {
+        return cj * __ldg(D + p * n + q) * __ldg(D + r * n + s) + ck * __ldg(D + p * n + r) * __ldg(D + q * n + s);
+    };
+    const double g[8] = {G(i, j, k, l), s12 ? G(j, i, k, l) : 0.0, s34 ? G(i, j, l, k) : 0.0,
+                         (s12 && s34) ? G(j, i, l, k) : 0.0, sPQ ? G(k, l, i, j) : 0.0,
+                         (sPQ && s34) ? G(l, k, i, j) : 0.0, (sPQ && s12) ? G(k, l, j, i) : 0.0,
+                         (sPQ && s12 && s34) ? G(l, k, j, i) : 0.0};
+    if (images) {
+        for (int m = 0; m < 8; ++m) gam[t * 8 + m] = g[m];
+    } else {
+        double s = 0.0;
+        for (int m = 0; m < 8; ++m) s += g[m];
+        gam[t] = s;
+    }
+}
+
+static int tile_check(qx_handle* h, int cls, long long q0, long long q1) {
+    if (!h || cls < 0 || cls >= QX_NCLS_ALL) return fail(QX_E_INVALID, "derivative tile: bad handle or class");
+    const ClassWork& w = h->work[cls];
+    if (q0 < 0 || q1 < q0 || q1 > w.nq) return fail(QX_E_INVALID, "derivative tile: quartet range %lld..%lld of %lld", q0, q1, w.nq);
+    return QX_OK;
+}
+
+extern "C" int qx_deriv_tile(qx_handle* h, int cls, long long q0, long long q1, int images, double* B, long long E,
+                             void* stream) {
+    int rc = tile_check(h, cls, q0, q1);
+    if (rc) return rc;
+    if (!B) return fail(QX_E_INVALID, "qx_deriv_tile: NULL buffer");
+    const long long need = (q1 - q0) * g_class_nout[cls] * (images ? 8 : 1);
+    if (E < need) return fail(QX_E_INVALID, "qx_deriv_tile: row length %lld < %lld elements", E, need);
+    if (q1 == q0) return QX_OK;
+    DeviceGuard g(h->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const ClassWork& w = h->work[cls];
+    EriArgs a = class_args(h, cls, B);
+    a.quartets = w.d_q + q0;
+    a.nq = q1 - q0;
+    a.nq64 = w.nq64 >= q1 ? a.nq : std::max(0LL, w.nq64 - q0);
+    if (h->deriv_eng[cls] == ENG_WARP) {
+        WarpArgs wa;
+        wa.e = a;
+        wa.wpq = h->wpq_deriv[cls];
+        wa.D = nullptr;
+        wa.cj = wa.ck = 0.0;
+        wa.grad = nullptr;
+        wa.slice = -1;
+        wa.tile_E = E;
+        wa.tile_images = images;
+        g_warp_deriv[cls](wa, WMODE_DER_TILE, s);
+    } else {  // the Rys engine serves every class (the split-mode engines have no tile epilogue)
+        RysArgs ra;
+        ra.e = a;
+        ra.rys = h->d_rys;
+        ra.M = 3 * h->natom;
+        ra.tile_E = E;
+        ra.tile_images = images;
+        if (g_rys_launch[cls](ra, RK_GRADT, 0, a.nq, s)) return rys_unsupported(cls, "derivative-tile");
+    }
+    QX_CUDA(cudaGetLastError());
+    return QX_OK;
+}
+
+extern "C" int qx_gamma_tile(qx_handle* h, int cls, long long q0, long long q1, int images, const double* D,
+                             double cj, double ck, double* gam, void* stream) {
+    int rc = tile_check(h, cls, q0, q1);
+    if (rc) return rc;
+    if (!D || !gam) return fail(QX_E_INVALID, "qx_gamma_tile: NULL argument");
+    if (q1 == q0) return QX_OK;
+    DeviceGuard g(h->device);
+    const ClassWork& w = h->work[cls];
+    const int* L = g_class_l[cls];
+    const int nb = (L[1] + 1) * (L[1] + 2) / 2, nc = (L[2] + 1) * (L[2] + 2) / 2, nd = (L[3] + 1) * (L[3] + 2) / 2;
+    const long long tot = (q1 - q0) * g_class_nout[cls];
+    k_gamma_tile<<<(unsigned)((tot + 127) / 128), 128, 0, (cudaStream_t)stream>>>(
+        w.d_q + q0, q1 - q0, h->d_pairs, nb, nc, nd, g_class_nout[cls], D, h->nbf, cj, ck, images, gam);
+    QX_CUDA(cudaGetLastError());
+    return QX_OK;
+}
+
 // ---------------------------------------------------------------- direct J/K ---
 // max |D| over each pair record's block (one warp per pair record)
 __global__ void __launch_bounds__(128) k_pair_dmax(const PairInfo* __restrict__ pairs, int npair,

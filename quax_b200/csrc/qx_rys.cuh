@@ -48,7 +48,8 @@ constexpr int RYS_TABLE_DOUBLES = QX_RYS_TAB_SIZE + 2 * QX_RYS_ASYM_SIZE;
 // Kinds of Rys programs: which centres are raised for derivatives, the
 // derivative order the quadrature must integrate, and the per-direction 1-D
 // derivative tables the products read.
-enum { RK_PLAIN = 0, RK_GRAD = 1, RK_HVP = 2, RK_DER1 = 11, RK_DER2 = 12, RK_DER3 = 13, RK_DER4 = 14 };
+enum { RK_PLAIN = 0, RK_GRAD = 1, RK_HVP = 2, RK_GRADT = 3, RK_DER1 = 11, RK_DER2 = 12, RK_DER3 = 13,
+       RK_DER4 = 14 };
 // Epilogues of the plain kind (the derivative kinds have their own).
 enum { RMODE_DENSE = 0, RMODE_UNIQUE = 1, RMODE_SCHWARZ = 2, RMODE_JK = 3 };
 
@@ -71,6 +72,10 @@ struct RysKind<RK_PLAIN> {
 };
 template <>
 struct RysKind<RK_GRAD> {  // A, B, C raised by one; tables I, dA, dB, dC (D by invariance)
+    static constexpr int ORD = 1, KA = 1, KB = 1, KC = 1, KD = 0, NOPS = 4;
+};
+template <>
+struct RysKind<RK_GRADT> {  // as RK_GRAD, but the 9 derivative integrals are written to a tile
     static constexpr int ORD = 1, KA = 1, KB = 1, KC = 1, KD = 0, NOPS = 4;
 };
 template <>
@@ -101,8 +106,9 @@ struct RysCls {
     static constexpr int SZ0 = (LA + 1) * (LB + 1) * (LC + 1) * (LD + 1);
     static constexpr int NOPS = K::NOPS;
     static constexpr int UOPS = NOPS * SZ0;
-    // team size: about 12 components per thread, 32..256 threads
-    static constexpr int TS0 = (NCOMP + 11) / 12;
+    // team size: about 12 components per thread (8 for the gradient tile, which
+    // keeps 9 sums per component), 32..256 threads
+    static constexpr int TS0 = KIND == RK_GRADT ? (NCOMP + 7) / 8 : (NCOMP + 11) / 12;
     static constexpr int TS = TS0 <= 32 ? 32 : TS0 <= 64 ? 64 : TS0 <= 128 ? 128 : 256;
     static constexpr int BS = TS < 128 ? 128 : TS;
     static constexpr int TPB = BS / TS;
@@ -118,6 +124,8 @@ struct RysCls {
     static_assert((KIND != RK_PLAIN || SRAW < 1024) && SZ0 < 1024, "1-D table offsets exceed 10 bits");
     // derivative tensors: multi-indices accumulated per pass over the primitives
     static constexpr int MG = NCPT >= 32 ? 1 : (32 / NCPT > 8 ? 8 : 32 / NCPT);
+    // gradient tile: derivative coordinates (of the 9) accumulated per pass
+    static constexpr int GG = NCPT * 9 <= 72 ? 9 : (72 / NCPT < 1 ? 1 : 72 / NCPT);
 };
 
 struct RysArgs {
@@ -134,6 +142,10 @@ struct RysArgs {
     int nchunk = 1;               // work items per quartet
     int slice_k = 0;              // 0: dense; else the slice's order (== k)
     int slice_nu[4] = {0, 0, 0, 0};  // the slice's sorted nuclear indices
+    // first-derivative tile (RK_DER1 only): out is a (3N, tile_E) row-major
+    // buffer with the layout of the warp kernels' WMODE_DER_TILE
+    long long tile_E = 0;
+    int tile_images = 0;
 };
 
 // ------------------------------------------------------------ nodes, weights ---
@@ -371,33 +383,81 @@ QX_HD inline void rys_phase_ops(const RysPrim& s, int nrb, double* U, double* O,
         const int d = el % (LD + 1), c = (el / (LD + 1)) % (LC + 1), b = (el / ((LD + 1) * (LC + 1))) % (LB + 1),
                   a = el / ((LD + 1) * (LC + 1) * (LB + 1));
         double v;
-        if constexpr (KIND == RK_GRAD) {
-            int k[4] = {0, 0, 0, 0};
-            if (op) k[op - 1] = 1;
-            v = rys_op_value<C>(s, U, u, k, a, b, c, d);
+        if constexpr (KIND == RK_GRAD || KIND == RK_GRADT) {
+            // closed forms: I, and dX g = 2 e_X g(x+1) - x g(x-1) for X = A, B, C
+            auto R = [&](int ia, int ib, int ic) { return rys_gk<C>(U, u, ia, ib, d, ic); };
+            if (op == 0) {
+                v = R(a, b, c);
+            } else if (op == 1) {
+                v = s.e2[0] * R(a + 1, b, c) - (a ? a * R(a - 1, b, c) : 0.0);
+            } else if (op == 2) {
+                v = s.e2[1] * R(a, b + 1, c) - (b ? b * R(a, b - 1, c) : 0.0);
+            } else {
+                v = s.e2[2] * R(a, b, c + 1) - (c ? c * R(a, b, c - 1) : 0.0);
+            }
         } else if constexpr (KIND == RK_HVP) {
+            // first and second derivatives on A, B, C in closed form: per centre the
+            // index shifts by +-1 (+-2 for a repeated centre) with the factors of
+            // d g_i = e2 g_{i+1} - i g_{i-1}
             const int x = u % 3;
-            if (op < 4) {
-                int k[4] = {0, 0, 0, 0};
-                if (op) k[op - 1] = 1;
-                v = rys_op_value<C>(s, U, u, k, a, b, c, d);
-            } else if (op == 4) {
-                v = 0.0;
-                for (int X = 0; X < 3; ++X) {
-                    int k[4] = {0, 0, 0, 0};
-                    k[X] = 1;
-                    v += w9[3 * X + x] * rys_op_value<C>(s, U, u, k, a, b, c, d);
+            const int idx0[3] = {a, b, c};
+            auto R = [&](const int* ix) { return rys_gk<C>(U, u, ix[0], ix[1], d, ix[2]); };
+            auto d1 = [&](int X) {  // dX I
+                int ix[3] = {a, b, c};
+                ix[X] += 1;
+                double r = s.e2[X] * R(ix);
+                if (idx0[X]) {
+                    ix[X] -= 2;
+                    r -= idx0[X] * R(ix);
                 }
+                return r;
+            };
+            auto d2 = [&](int X, int Y) {  // dX dY I
+                int ix[3] = {a, b, c};
+                if (X == Y) {
+                    const int i = idx0[X];
+                    ix[X] = i + 2;
+                    double r = s.e2[X] * s.e2[X] * R(ix);
+                    ix[X] = i;
+                    r -= s.e2[X] * (2 * i + 1) * R(ix);
+                    if (i >= 2) {
+                        ix[X] = i - 2;
+                        r += (double)(i * (i - 1)) * R(ix);
+                    }
+                    return r;
+                }
+                double r = 0.0;
+                for (int sx = 0; sx < 2; ++sx)
+                    for (int sy = 0; sy < 2; ++sy) {
+                        const int ixx = idx0[X] + (sx ? -1 : 1), iyy = idx0[Y] + (sy ? -1 : 1);
+                        if (ixx < 0 || iyy < 0) continue;
+                        const double cf = (sx ? -(double)idx0[X] : s.e2[X]) * (sy ? -(double)idx0[Y] : s.e2[Y]);
+                        int jx[3] = {a, b, c};
+                        jx[X] = ixx;
+                        jx[Y] = iyy;
+                        r += cf * R(jx);
+                    }
+                return r;
+            };
+            if (op == 0) {
+                v = R(idx0);
+            } else if (op < 4) {
+                v = d1(op - 1);
+            } else if (op == 4) {
+                v = w9[x] * d1(0) + w9[3 + x] * d1(1) + w9[6 + x] * d1(2);
             } else {
                 const int Y = op - 5;
-                v = 0.0;
-                for (int X = 0; X < 3; ++X) {
-                    int k[4] = {0, 0, 0, 0};
-                    k[X] += 1;
-                    k[Y] += 1;
-                    v += w9[3 * X + x] * rys_op_value<C>(s, U, u, k, a, b, c, d);
-                }
+                v = w9[x] * d2(0, Y) + w9[3 + x] * d2(1, Y) + w9[6 + x] * d2(2, Y);
             }
+        } else if constexpr (C::K::ORD == 1) {
+            // order 1, all four centres raised: ops in rys_op_rank order are
+            // I, dD, dC, dB, dA, in closed form
+            auto R = [&](int ia, int ib, int ic, int id) { return rys_gk<C>(U, u, ia, ib, id, ic); };
+            if (op == 0) v = R(a, b, c, d);
+            else if (op == 1) v = s.e2[3] * R(a, b, c, d + 1) - (d ? d * R(a, b, c, d - 1) : 0.0);
+            else if (op == 2) v = s.e2[2] * R(a, b, c + 1, d) - (c ? c * R(a, b, c - 1, d) : 0.0);
+            else if (op == 3) v = s.e2[1] * R(a, b + 1, c, d) - (b ? b * R(a, b - 1, c, d) : 0.0);
+            else v = s.e2[0] * R(a + 1, b, c, d) - (a ? a * R(a - 1, b, c, d) : 0.0);
         } else {
             constexpr int K = C::K::ORD;
             // unrank op within tuples of sum <= K (lexicographic)
@@ -472,6 +532,29 @@ QX_HD inline void rys_prod_grad(const double* O, int nrb, int off, double gam, d
             g[3 * c + 0] = fma(X[(c + 1) * S + ox], yz, g[3 * c + 0]);
             g[3 * c + 1] = fma(Y[(c + 1) * S + oy], xz, g[3 * c + 1]);
             g[3 * c + 2] = fma(Z[(c + 1) * S + oz], xy, g[3 * c + 2]);
+        }
+    }
+}
+
+// Gradient-tile kind: acc[b - b0] += sum_r (dX I)_i prod_{j != i} I_j for the
+// derivative coordinates b = 3X + i in [b0, b0 + GG).
+template <class C>
+QX_HD inline void rys_prod_gradt(const double* O, int nrb, int off, int b0, double* acc) {
+    const int o[3] = {off & 1023, (off >> 10) & 1023, off >> 20};
+    constexpr int S = C::SZ0;
+    for (int r = 0; r < nrb; ++r) {
+        const double* T[3];
+        T[0] = O + (size_t)3 * r * C::UOPS;
+        T[1] = T[0] + C::UOPS;
+        T[2] = T[1] + C::UOPS;
+        const double I[3] = {T[0][o[0]], T[1][o[1]], T[2][o[2]]};
+#pragma unroll
+        for (int g = 0; g < C::GG; ++g) {
+            const int b = b0 + g;
+            if (b >= 9) break;
+            const int X = b / 3, i = b - 3 * X;
+            const double other = i == 0 ? I[1] * I[2] : (i == 1 ? I[0] * I[2] : I[0] * I[1]);
+            acc[g] = fma(T[i][(X + 1) * S + o[i]], other, acc[g]);
         }
     }
 }
@@ -792,6 +875,41 @@ __global__ void __launch_bounds__(RysCls<LA, LB, LC, LD, KIND>::BS)
                 else
                     dense_images(a.out, n, ii, jj, kk, ll, s12, s34, sPQ, acc[j]);
             }
+        } else if constexpr (KIND == RK_GRADT) {
+            // the first-derivative integrals of the quartet, summed over primitives in
+            // registers (GG coordinates per pass), then added into the tile: centre X's
+            // block to its atom's rows, minus the sum to the D centre's atom
+            constexpr int GG = C::GG;
+            for (int b0 = 0; b0 < 9; b0 += GG) {
+                double acc[NCPT][GG];
+#pragma unroll
+                for (int j = 0; j < NCPT; ++j)
+#pragma unroll
+                    for (int g = 0; g < GG; ++g) acc[j][g] = 0.0;
+                for (int t = 0; t < ntot; ++t) {
+                    const int i = t / nk, jj = t - i * nk;
+                    rys_primitive<C, KIND, LA, LB, LC, LD>(ra, a.prims[P.prim_off + i], a.prims[Q.prim_off + jj], P,
+                                                            Q, uw, U, O, w9, tid, team, [&](int nrb) {
+#pragma unroll
+                        for (int j = 0; j < NCPT; ++j)
+                            if (tid + j * TS < C::NCOMP) rys_prod_gradt<C>(O, nrb, offs[j], b0, acc[j]);
+                    });
+                }
+#pragma unroll
+                for (int j = 0; j < NCPT; ++j) {
+                    const int kc = tid + j * TS;
+                    if (kc >= C::NCOMP) continue;
+                    const long long e = qi * C::NCOMP + kc;
+#pragma unroll
+                    for (int g = 0; g < GG; ++g) {
+                        const int b = b0 + g;
+                        if (b >= 9) break;
+                        const int X = b / 3, x = b - 3 * X;
+                        tile_add(a.out, ra.tile_E, 3 * atoms[X] + x, e, ra.tile_images, s12, s34, sPQ, acc[j][g]);
+                        tile_add(a.out, ra.tile_E, 3 * atoms[3] + x, e, ra.tile_images, s12, s34, sPQ, -acc[j][g]);
+                    }
+                }
+            }
         } else if constexpr (KIND == RK_GRAD || KIND == RK_HVP) {
             double g[9];
 #pragma unroll
@@ -853,8 +971,12 @@ __global__ void __launch_bounds__(RysCls<LA, LB, LC, LD, KIND>::BS)
                     for (int mm = 0; mm < mn; ++mm) {
                         const double mult = mmult[m0 + mm];
                         if (mult == 0.0) continue;
-                        atomic_images_w(a.out + mslot[m0 + mm] * n4, n, ii, jj, kk, ll, s12, s34, sPQ,
-                                        mult * acc[j][mm]);
+                        if (ra.tile_E)  // order 1: the slot is the nuclear index
+                            tile_add(a.out, ra.tile_E, (int)mslot[m0 + mm], qi * C::NCOMP + kc, ra.tile_images, s12,
+                                     s34, sPQ, mult * acc[j][mm]);
+                        else
+                            atomic_images_w(a.out + mslot[m0 + mm] * n4, n, ii, jj, kk, ll, s12, s34, sPQ,
+                                            mult * acc[j][mm]);
                     }
                 }
             }

@@ -27,10 +27,38 @@ struct WarpArgs {
     // split mode: the quartets' accumulators (NITEM_PAD per quartet, item order)
     // were summed by k_gvrr; the kernel runs only the HRR and the epilogue
     const double* acc_in = nullptr;
+    // derivative tile (WMODE_DER_TILE): out is a (3N, tile_E) row-major buffer,
+    // element qi * NOUT + o (tile_images = 0), or (qi * NOUT + o) * 8 + image for
+    // each distinct image of the integral (tile_images = 1)
+    long long tile_E = 0;
+    int tile_images = 0;
 };
 
 enum { WMODE_DENSE = 0, WMODE_UNIQUE = 1, WMODE_SCHWARZ = 2, WMODE_DER_DENSE = 10, WMODE_DER_SLICE = 11,
-       WMODE_GRAD = 12, WMODE_DER2_DENSE = 13, WMODE_DER2_SLICE = 14, WMODE_HVP = 15 };
+       WMODE_GRAD = 12, WMODE_DER2_DENSE = 13, WMODE_DER2_SLICE = 14, WMODE_HVP = 15, WMODE_DER_TILE = 16 };
+
+// Adds v to row `row` of a derivative tile at element e of quartet-local index:
+// once (unique elements) or into the slot of every distinct image (8 per element;
+// the images (ij|kl), (ji|kl), (ij|lk), (ji|lk), (kl|ij), (lk|ij), (kl|ji), (lk|ji)).
+__device__ __forceinline__ void tile_add(double* __restrict__ B, long long E, int row, long long e, bool images,
+                                         bool s12, bool s34, bool sPQ, double v) {
+    double* r = B + (long long)row * E;
+    if (!images) {
+        atomicAdd(r + e, v);
+        return;
+    }
+    double* b = r + e * 8;
+    atomicAdd(b + 0, v);
+    if (s12) atomicAdd(b + 1, v);
+    if (s34) atomicAdd(b + 2, v);
+    if (s12 && s34) atomicAdd(b + 3, v);
+    if (sPQ) {
+        atomicAdd(b + 4, v);
+        if (s34) atomicAdd(b + 5, v);
+        if (s12) atomicAdd(b + 6, v);
+        if (s12 && s34) atomicAdd(b + 7, v);
+    }
+}
 
 constexpr int WARP_QPB = 4;  // quartets (warps) per block
 
@@ -540,6 +568,12 @@ __global__ void __launch_bounds__(WARP_QPB * 32) k_warp(WarpArgs wa, int mode) {
         const int id = o % ND, ic = (o / ND) % NC, ib = (o / (ND * NC)) % NB, ia = o / (ND * NC * NB);
         const long long ii = P.bf1 + ia, jj = P.bf2 + ib, kk = Q.bf1 + ic, ll = Q.bf2 + id;
         const int sp = 3 * atc + xyz, sm = 3 * atD + xyz;
+        if (mode == WMODE_DER_TILE) {
+            const long long e = qi * W::NOUT + o;
+            tile_add(a.out, wa.tile_E, sp, e, wa.tile_images, s12, s34, sPQ, v);
+            tile_add(a.out, wa.tile_E, sm, e, wa.tile_images, s12, s34, sPQ, -v);
+            return;
+        }
         if (mode == WMODE_DER_DENSE) {
             atomic_images_w(a.out + (long long)sp * n4, n, ii, jj, kk, ll, s12, s34, sPQ, v);
             atomic_images_w(a.out + (long long)sm * n4, n, ii, jj, kk, ll, s12, s34, sPQ, -v);

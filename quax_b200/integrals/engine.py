@@ -314,6 +314,44 @@ class EriEngine:
             )
         return out
 
+    def grad_plain(self, D: torch.Tensor, cj: float = 1.0, ck: float = -0.5, images: bool = True,
+                   tile_bytes: int = 2 << 30, stream=None) -> torch.Tensor:
+        """The plain FP64 derivative-tensor path for sum Gamma dG/dR (3N vector):
+        class by class, tiles of unique quartets have their first-derivative
+        integrals materialised as a (3N, tile) tensor -- with images=True every
+        distinct image of each integral, i.e. the elements of the reference's
+        dense (3N, n^4) tensor -- and then contracted with Gamma in one GEMV per
+        tile.  Each derivative quartet is evaluated once.  Tiles hold at most
+        tile_bytes of derivative tensor."""
+        D = D.to(device=self.device, dtype=torch.float64).contiguous()
+        M = 3 * self.natom
+        width = 8 if images else 1
+        info = [c for c in self.class_info() if c["nq"]]
+        largest = max((int(np.prod([(l + 1) * (l + 2) // 2 for l in c["l"]])) for c in info), default=1) * width
+        emax = max(largest, tile_bytes // (8 * M))  # at least one quartet per tile
+        B = torch.empty(M * emax, dtype=torch.float64, device=self.device)
+        gam = torch.empty(emax, dtype=torch.float64, device=self.device)
+        g = torch.zeros(M, dtype=torch.float64, device=self.device)
+        lib = _lib.load()
+        sp = C.c_void_p(_stream_ptr(stream))
+        with torch.cuda.device(self.device):
+            for c in info:
+                nq = c["nq"]
+                ncomp = int(np.prod([(l + 1) * (l + 2) // 2 for l in c["l"]]))
+                qt = max(1, emax // (ncomp * width))
+                for q0 in range(0, nq, qt):
+                    q1 = min(nq, q0 + qt)
+                    E = (q1 - q0) * ncomp * width
+                    Bv = B[: M * E].view(M, E)
+                    Bv.zero_()
+                    _lib.check(lib.qx_deriv_tile(self.handle, c["cls"], q0, q1, int(images),
+                                                 C.c_void_p(Bv.data_ptr()), E, sp), "qx_deriv_tile")
+                    _lib.check(lib.qx_gamma_tile(self.handle, c["cls"], q0, q1, int(images),
+                                                 C.c_void_p(D.data_ptr()), float(cj), float(ck),
+                                                 C.c_void_p(gam.data_ptr()), sp), "qx_gamma_tile")
+                    g += Bv @ gam[:E]
+        return g
+
     # -- Fock-matrix pieces -----------------------------------------------------
     def jk(self, D: torch.Tensor, J: torch.Tensor | None = None, K: torch.Tensor | None = None, stream=None,
            screen: float = 0.0):
