@@ -271,9 +271,12 @@ int qx_gamma_tile(qx_handle *h, int cls, long long q0, long long q1, int images,
  * returns when the tensor is complete.  A basis whose tables do not fit (about
  * 1.5 million screened unique quartets) is rejected with QX_E_INVALID.  All calls
  * share the array, which keeps the previous call's contents, so calls that overlap
- * on the GPU race and must be serialised by the caller.  The first call on a device
- * looks up the array's address and uploads a constant table synchronously; make it
- * before any stream capture.  Errors are reported through qx_last_error(). */
+ * on the GPU race and must be serialised by the caller.  Every call blocks the host
+ * (it reads the Schwarz values back and returns when the tensor is complete), so it
+ * cannot be recorded into a CUDA graph: on a stream that is capturing it returns
+ * QX_E_INVALID.  The first call on a device looks up the array's address and
+ * uploads a constant table synchronously.  Shells up to d (l <= 2).  Errors are
+ * reported through qx_last_error(). */
 int qx_compute_2e_int_noalloc(int natom, const double *coords, int nshell, const int *shell_l,
                               const int *shell_nprim, const int *shell_atom, const double *exps,
                               const double *coefs, double ints_tol, double *out_dev, void *stream);

@@ -2,9 +2,12 @@
 # Compiles the reference's own index helpers (quax/integrals/utils.h, read in
 # place from the reference tree) with oracle/ref_utils_shim.cpp into
 # oracle/_ref/libquax_ref_utils.so.  Test infrastructure only.
+# Usage: build_ref.sh [REFERENCE_ROOT]
+#   REFERENCE_ROOT: the argument, else $QUAX_REFERENCE, else the checkout this
+#   oracle was pinned against (/root/reference); without one, nothing is built.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${QUAX_REFERENCE:-/root/reference}"
+REF="${1:-${QUAX_REFERENCE:-/root/reference}}"
 HDR="$REF/quax/integrals/utils.h"
 if [ ! -f "$HDR" ]; then
   echo "reference header $HDR not found; nothing built" >&2

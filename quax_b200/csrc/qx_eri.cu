@@ -31,6 +31,7 @@
 #include "quax_b200.h"
 #include "qx_warp.cuh"
 #include "qx_rys.cuh"
+#include "qx_setup.h"
 #include "gen/warp_index.cuh"
 #include "gen/rys_index.cuh"
 
@@ -192,43 +193,6 @@ static bool init_class_tables() {
     return true;
 }
 static const bool g_tables_ready = init_class_tables();
-
-// ------------------------------------------------------------------ Boys table --
-static void boys_table_compute(std::vector<double>& tab) {
-    tab.assign((size_t)BOYS_NG * BOYS_NM, 0.0);
-    for (int g = 0; g < BOYS_NG; ++g) {
-        const double T = g / BOYS_INV_H;
-        double F[BOYS_NM];
-        const int M = BOYS_NM - 1;
-        if (T == 0.0) {
-            for (int m = 0; m <= M; ++m) F[m] = 1.0 / (2 * m + 1);
-        } else {
-            // series at the top order, then downward recursion
-            long double term = 1.0L / (2 * M + 1), sum = term;
-            for (int k = 1; k < 4000; ++k) {
-                term *= 2.0L * T / (2 * M + 2 * k + 1);
-                sum += term;
-                if (term < sum * 1e-21L) break;
-            }
-            const long double eT = expl(-(long double)T);
-            long double Fm = eT * sum;
-            F[M] = (double)Fm;
-            for (int m = M; m > 0; --m) {
-                Fm = (2.0L * T * Fm + eT) / (2 * m - 1);
-                F[m - 1] = (double)Fm;
-            }
-        }
-        for (int m = 0; m < BOYS_NM; ++m) tab[(size_t)g * BOYS_NM + m] = F[m];
-    }
-}
-
-// The table depends on nothing but the grid: build it once per process.
-static void boys_table_host(std::vector<double>& tab) {
-    static std::once_flag once;
-    static std::vector<double> cached;
-    std::call_once(once, [] { boys_table_compute(cached); });
-    tab = cached;
-}
 
 // ------------------------------------------------------------------ handle ----
 struct ClassWork {
@@ -474,12 +438,6 @@ static void free_handle(qx_handle* h) {
     delete h;
 }
 
-static double dfact(int n) {
-    double r = 1.0;
-    while (n > 1) { r *= n; n -= 2; }
-    return r;
-}
-
 static int run_class(qx_handle* h, int cls, int mode, const int2* d_q, long long nq, double* out, long long n,
                      long long base, cudaStream_t s, int log2g = 0, double* scratch = nullptr, double* out2 = nullptr,
                      const double* dens = nullptr) {
@@ -583,97 +541,31 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
     h->pure = pure;
     h->tol = ints_tol;
     h->coords.assign(coords, coords + 3 * natom);
-    int off = 0, bf = 0;
-    for (int s = 0; s < nshell; ++s) {
-        const int l = shell_l[s], k = shell_nprim[s], at = shell_atom[s];
-        if (l < 0 || l > QX_RYS_LMAX) {
+    ShellTables shells;
+    {
+        std::string err;
+        const int rc = normalize_shells("qx_initialize", natom, nshell, shell_l, shell_nprim, shell_atom, exps, coefs,
+                                        QX_RYS_LMAX, shells, err);
+        if (rc) {
             free_handle(h);
-            return fail(QX_E_UNSUPPORTED, "qx_initialize: shell %d has l=%d (compiled max %d)", s, l, QX_RYS_LMAX);
+            return fail(rc, "%s", err.c_str());
         }
-        if (k <= 0 || k > 64) {
-            free_handle(h);
-            return fail(QX_E_INVALID, "qx_initialize: shell %d has %d primitives (1..64 allowed)", s, k);
-        }
-        if (at < 0 || at >= natom) {
-            free_handle(h);
-            return fail(QX_E_INVALID, "qx_initialize: shell %d on atom %d of %d", s, at, natom);
-        }
-        h->l.push_back(l);
-        h->nprim.push_back(k);
-        h->atom.push_back(at);
-        h->poff.push_back(off);
-        h->bf.push_back(bf);
-        for (int c = 0; c < 3; ++c) h->centers.push_back(coords[3 * at + c]);
-        // Libint-convention normalisation
-        const double df = dfact(2 * l - 1);
-        std::vector<double> c(k);
-        for (int p = 0; p < k; ++p) {
-            const double a = exps[off + p];
-            if (!(a > 0.0) || !std::isfinite(a) || !std::isfinite(coefs[off + p])) {
-                free_handle(h);
-                return fail(QX_E_INVALID, "qx_initialize: shell %d primitive %d has exponent %g", s, p, a);
-            }
-            c[p] = coefs[off + p] * std::sqrt(std::pow(2.0, l) * std::pow(2.0 * a, l + 1.5) / (std::pow(M_PI, 1.5) * df));
-        }
-        double nrm = 0.0;
-        for (int p = 0; p < k; ++p)
-            for (int q = 0; q < k; ++q)
-                nrm += c[p] * c[q] * df * std::pow(M_PI, 1.5) / (std::pow(2.0, l) * std::pow(exps[off + p] + exps[off + q], l + 1.5));
-        if (!(nrm > 0.0)) {
-            free_handle(h);
-            return fail(QX_E_INVALID, "qx_initialize: shell %d has a degenerate contraction", s);
-        }
-        for (int p = 0; p < k; ++p) {
-            h->alpha.push_back(exps[off + p]);
-            h->coef.push_back(c[p] / std::sqrt(nrm));
-        }
-        off += k;
-        bf += ncart_h(l);
     }
-    h->nbf = bf;
+    h->l = shells.l;
+    h->nprim = shells.nprim;
+    h->atom = shells.atom;
+    h->poff = shells.poff;
+    h->bf = shells.bf;
+    h->alpha = shells.alpha;
+    h->coef = shells.coef;
+    h->nbf = shells.nbf;
+    for (int s = 0; s < nshell; ++s)
+        for (int c = 0; c < 3; ++c) h->centers.push_back(coords[3 * shells.atom[s] + c]);
     trace.mark("shells");
     // pair records
     std::vector<PrimPair> prims;
-    const double kfac = std::sqrt(2.0) * std::pow(M_PI, 1.25);
-    for (int s1 = 0; s1 < nshell; ++s1)
-        for (int s2 = 0; s2 <= s1; ++s2) {
-            int f = s1, g = s2;
-            if (h->l[s2] > h->l[s1]) std::swap(f, g);
-            PairInfo pi;
-            const double* A = &h->centers[3 * f];
-            const double* B = &h->centers[3 * g];
-            pi.Ax = A[0]; pi.Ay = A[1]; pi.Az = A[2];
-            pi.ABx = A[0] - B[0]; pi.ABy = A[1] - B[1]; pi.ABz = A[2] - B[2];
-            const double AB2 = pi.ABx * pi.ABx + pi.ABy * pi.ABy + pi.ABz * pi.ABz;
-            pi.prim_off = (int)prims.size();
-            pi.nprim = h->nprim[f] * h->nprim[g];
-            pi.bf1 = h->bf[f]; pi.bf2 = h->bf[g];
-            pi.s1 = f; pi.s2 = g;
-            pi.atom1 = h->atom[f]; pi.atom2 = h->atom[g];
-            pi.l1 = h->l[f]; pi.l2 = h->l[g];
-            for (int p = 0; p < h->nprim[f]; ++p)
-                for (int q = 0; q < h->nprim[g]; ++q) {
-                    const double a = h->alpha[h->poff[f] + p], b = h->alpha[h->poff[g] + q];
-                    const double ca = h->coef[h->poff[f] + p], cb = h->coef[h->poff[g] + q];
-                    PrimPair r;
-                    r.zeta = a + b;
-                    r.oo2z = 0.5 / r.zeta;
-                    // P - A = -(b / zeta)(A - B), exactly zero for a one-centre pair (forming
-                    // P first and subtracting A leaves ~1e-15 there, which tight exponents
-                    // amplify beyond 1e-12 in integrals that vanish by symmetry)
-                    r.PAx = -(b / r.zeta) * (A[0] - B[0]);
-                    r.PAy = -(b / r.zeta) * (A[1] - B[1]);
-                    r.PAz = -(b / r.zeta) * (A[2] - B[2]);
-                    r.Px = A[0] + r.PAx; r.Py = A[1] + r.PAy; r.Pz = A[2] + r.PAz;
-                    r.K = kfac * ca * cb * std::exp(-a * b / r.zeta * AB2) / r.zeta;
-                    r.alpha = a;
-                    prims.push_back(r);
-                }
-            h->pairs.push_back(pi);
-            h->pcls.push_back(pair_class(pi.l1, pi.l2));
-        }
-    std::vector<double> boys;
-    boys_table_host(boys);
+    build_pairs(shells, coords, prims, h->pairs, h->pcls);
+    const std::vector<double>& boys = boys_table();
     const int np = (int)h->pairs.size();
     {
         // bulk-copy staging of the primitive pairs in the split-mode VRR kernels:
@@ -1058,6 +950,58 @@ static int run_all_classes(qx_handle* h, int mode, double* out, long long n, cud
     return QX_OK;
 }
 
+// Device staging of host outputs: one buffer per device, grown on demand and kept
+// for the life of the process, so a host-output call allocates nothing once the
+// buffer is large enough (the dense tensors are GBs: a cudaMalloc/cudaFree pair
+// per call cost up to a few hundred ms).  Calls that stage on the same device are
+// serialised by the device's lock, held until their copy-out completes.
+namespace {
+struct Staging {
+    std::mutex mu;
+    double* p = nullptr;
+    size_t cap = 0;  // doubles
+};
+constexpr int kStagingDevices = 64;
+Staging g_staging[kStagingDevices];
+}  // namespace
+
+// Returns the device's staging buffer with room for `count` doubles (lk must lock
+// the device's mutex), or nullptr when the device cannot provide it.
+static double* staging_get(int dev, size_t count, std::unique_lock<std::mutex>& lk) {
+    if (dev < 0 || dev >= kStagingDevices) return nullptr;
+    Staging& st = g_staging[dev];
+    lk = std::unique_lock<std::mutex>(st.mu);
+    if (st.cap < count) {
+        cudaFree(st.p);
+        st.p = nullptr;
+        st.cap = 0;
+        if (cudaMalloc((void**)&st.p, sizeof(double) * count) != cudaSuccess) {
+            cudaGetLastError();
+            st.p = nullptr;
+            return nullptr;
+        }
+        st.cap = count;
+    }
+    return st.p;
+}
+
+// Stages a host output buffer through the device when out_on_device == 0.
+template <class F>
+static int with_output(qx_handle* h, double* out, size_t count, int out_on_device, cudaStream_t s, F&& body) {
+    if (out_on_device) return body(out);
+    std::unique_lock<std::mutex> lk;
+    double* d = staging_get(h->device, count, lk);
+    if (!d) return fail(QX_E_NOMEM, "cannot stage %zu bytes on the device", sizeof(double) * count);
+    int rc = body(d);
+    if (!rc) {
+        cudaError_t e = cudaMemcpyAsync(out, d, sizeof(double) * count, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) rc = fail(QX_E_CUDA, "copy-out failed: %s", cudaGetErrorString(e));
+    }
+    if (!rc) rc = check_err_word(h, s);
+    return rc;
+}
+
 static int eri_dense_dev(qx_handle* h, double* out, cudaStream_t s) {
     const long long n = h->nbf;
     QX_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * n * n * n * n, s));
@@ -1069,22 +1013,7 @@ extern "C" int qx_compute_2e_int(qx_handle* h, double* out, int out_on_device, v
     DeviceGuard g(h->device);
     cudaStream_t s = (cudaStream_t)stream;
     const long long n = h->nbf;
-    const size_t bytes = sizeof(double) * (size_t)(n * n * n * n);
-    if (out_on_device) return eri_dense_dev(h, out, s);
-    double* d = nullptr;
-    if (cudaMalloc((void**)&d, bytes) != cudaSuccess) {
-        cudaGetLastError();
-        return fail(QX_E_NOMEM, "qx_compute_2e_int: cannot stage %zu bytes on the device", bytes);
-    }
-    int rc = eri_dense_dev(h, d, s);
-    if (!rc) {
-        cudaError_t e = cudaMemcpyAsync(out, d, bytes, cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess) rc = fail(QX_E_CUDA, "qx_compute_2e_int: %s", cudaGetErrorString(e));
-    }
-    cudaFree(d);
-    if (!rc) rc = check_err_word(h, s);
-    return rc;
+    return with_output(h, out, (size_t)(n * n * n * n), out_on_device, s, [&](double* d) { return eri_dense_dev(h, d, s); });
 }
 
 extern "C" int qx_eri_unique(qx_handle* h, double* out_dev, void* stream) {
@@ -1311,26 +1240,6 @@ static int run_all_derk(qx_handle* h, int k, double* out, const int* nu, cudaStr
         QX_CUDA(cudaStreamWaitEvent(s, h->done[i], 0));
     }
     return QX_OK;
-}
-
-// Stages a host output buffer through the device when out_on_device == 0.
-template <class F>
-static int with_output(qx_handle* h, double* out, size_t count, int out_on_device, cudaStream_t s, F&& body) {
-    if (out_on_device) return body(out);
-    double* d = nullptr;
-    if (cudaMalloc((void**)&d, sizeof(double) * count) != cudaSuccess) {
-        cudaGetLastError();
-        return fail(QX_E_NOMEM, "cannot stage %zu bytes on the device", sizeof(double) * count);
-    }
-    int rc = body(d);
-    if (!rc) {
-        cudaError_t e = cudaMemcpyAsync(out, d, sizeof(double) * count, cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess) rc = fail(QX_E_CUDA, "copy-out failed: %s", cudaGetErrorString(e));
-    }
-    cudaFree(d);
-    if (!rc) rc = check_err_word(h, s);
-    return rc;
 }
 
 extern "C" int qx_eri_deriv_core(qx_handle* h, int order, double* out, int out_on_device, void* stream) {

@@ -20,9 +20,12 @@
 //   * every call reuses the same array and it keeps the last call's contents;
 //     calls that overlap on the GPU (other streams, other host threads) race on
 //     it and must be serialised by the caller;
+//   * every call blocks the host: it reads the Schwarz values back to build the
+//     screened lists and returns once the tensor is complete, so no call can be
+//     recorded into a CUDA graph; a call on a stream that is capturing is refused
+//     with QX_E_INVALID (an XLA handler must be registered as not capturable);
 //   * the first call on a device looks up the array's device address and uploads
-//     the Boys table, synchronously; make that first call before any stream
-//     capture.
+//     the Boys table, synchronously.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -35,6 +38,7 @@
 
 #include "quax_b200.h"
 #include "qx_kernels.cuh"
+#include "qx_setup.h"
 
 using namespace qx;
 
@@ -57,7 +61,6 @@ int nofail(int code, const char* fmt, ...) {
     return code;
 }
 
-constexpr int pair_cls(int l1, int l2) { return l1 * (l1 + 1) / 2 + l2; }
 constexpr int quartet_cls(int pb, int pk) { return pb * (pb + 1) / 2 + pk; }
 constexpr size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 constexpr size_t kBoysBytes = sizeof(double) * BOYS_NG * BOYS_NM;
@@ -80,38 +83,6 @@ struct DeviceState {
 std::mutex g_mtx;
 DeviceState g_state[256];
 
-// Boys table, built once on the host (same construction as the handle path).
-const std::vector<double>& boys_host() {
-    static std::vector<double> tab = [] {
-        std::vector<double> t((size_t)BOYS_NG * BOYS_NM);
-        for (int g = 0; g < BOYS_NG; ++g) {
-            const double T = g / BOYS_INV_H;
-            const int M = BOYS_NM - 1;
-            double F[BOYS_NM];
-            if (T == 0.0) {
-                for (int m = 0; m <= M; ++m) F[m] = 1.0 / (2 * m + 1);
-            } else {
-                long double term = 1.0L / (2 * M + 1), sum = term;
-                for (int k = 1; k < 4000; ++k) {
-                    term *= 2.0L * T / (2 * M + 2 * k + 1);
-                    sum += term;
-                    if (term < sum * 1e-21L) break;
-                }
-                const long double eT = expl(-(long double)T);
-                long double Fm = eT * sum;
-                F[M] = (double)Fm;
-                for (int m = M; m > 0; --m) {
-                    Fm = (2.0L * T * Fm + eT) / (2 * m - 1);
-                    F[m - 1] = (double)Fm;
-                }
-            }
-            for (int m = 0; m < BOYS_NM; ++m) t[(size_t)g * BOYS_NM + m] = F[m];
-        }
-        return t;
-    }();
-    return tab;
-}
-
 // One-time set-up per device, with that device current.
 int setup_device(int dev) {
     std::lock_guard<std::mutex> lk(g_mtx);
@@ -122,7 +93,7 @@ int setup_device(int dev) {
     cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
     if (e != cudaSuccess)
         return nofail(QX_E_CUDA, "qx_compute_2e_int_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
-    const auto& tab = boys_host();
+    const auto& tab = boys_table();
     e = cudaMemcpy(ptr, tab.data(), kBoysBytes, cudaMemcpyHostToDevice);
     // a pageable host-to-device copy can still be in flight when cudaMemcpy returns;
     // the caller's stream may not order after it, so wait here (set-up only)
@@ -165,84 +136,30 @@ extern "C" int qx_compute_2e_int_noalloc(int natom, const double* coords, int ns
         return nofail(QX_E_INVALID, "qx_compute_2e_int_noalloc: ints_tol must be > 0");
     for (int i = 0; i < 3 * natom; ++i)
         if (!std::isfinite(coords[i])) return nofail(QX_E_INVALID, "qx_compute_2e_int_noalloc: non-finite coordinate");
-    // --- host tables (same construction as qx_initialize) ---
-    std::vector<int> l(nshell), nprim(nshell), atom(nshell), poff(nshell), bf(nshell);
-    std::vector<double> alpha, coef;
-    int off = 0, nbf = 0;
-    for (int s = 0; s < nshell; ++s) {
-        l[s] = shell_l[s];
-        nprim[s] = shell_nprim[s];
-        atom[s] = shell_atom[s];
-        if (l[s] < 0 || l[s] > QX_GEN_LMAX)
-            return nofail(QX_E_UNSUPPORTED, "qx_compute_2e_int_noalloc: shell %d has l=%d (max %d)", s, l[s], QX_GEN_LMAX);
-        if (nprim[s] <= 0 || nprim[s] > 64)
-            return nofail(QX_E_INVALID, "qx_compute_2e_int_noalloc: shell %d has %d primitives", s, nprim[s]);
-        if (atom[s] < 0 || atom[s] >= natom)
-            return nofail(QX_E_INVALID, "qx_compute_2e_int_noalloc: shell %d on atom %d", s, atom[s]);
-        poff[s] = off;
-        bf[s] = nbf;
-        double df = 1.0;
-        for (int k = 2 * l[s] - 1; k > 1; k -= 2) df *= k;
-        std::vector<double> c(nprim[s]);
-        for (int p = 0; p < nprim[s]; ++p) {
-            const double a = exps[off + p];
-            if (!(a > 0.0) || !std::isfinite(a) || !std::isfinite(coefs[off + p]))
-                return nofail(QX_E_INVALID, "qx_compute_2e_int_noalloc: shell %d primitive %d has exponent %g", s, p, a);
-            c[p] = coefs[off + p] * std::sqrt(std::pow(2.0, l[s]) * std::pow(2.0 * a, l[s] + 1.5) / (std::pow(M_PI, 1.5) * df));
+    {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing((cudaStream_t)stream, &cs) != cudaSuccess) {
+            cudaGetLastError();
+            return nofail(QX_E_INVALID, "qx_compute_2e_int_noalloc: cannot query the stream's capture state");
         }
-        double nrm = 0.0;
-        for (int p = 0; p < nprim[s]; ++p)
-            for (int q = 0; q < nprim[s]; ++q)
-                nrm += c[p] * c[q] * df * std::pow(M_PI, 1.5) /
-                       (std::pow(2.0, l[s]) * std::pow(exps[off + p] + exps[off + q], l[s] + 1.5));
-        if (!(nrm > 0.0)) return nofail(QX_E_INVALID, "qx_compute_2e_int_noalloc: degenerate contraction in shell %d", s);
-        for (int p = 0; p < nprim[s]; ++p) {
-            alpha.push_back(exps[off + p]);
-            coef.push_back(c[p] / std::sqrt(nrm));
-        }
-        off += nprim[s];
-        nbf += (l[s] + 1) * (l[s] + 2) / 2;
+        if (cs != cudaStreamCaptureStatusNone)
+            return nofail(QX_E_INVALID,
+                          "qx_compute_2e_int_noalloc: the stream is capturing; this call synchronises and cannot be "
+                          "recorded into a CUDA graph");
     }
+    // --- host tables (shared with qx_initialize) ---
+    ShellTables shells;
+    {
+        std::string err;
+        const int rc = normalize_shells("qx_compute_2e_int_noalloc", natom, nshell, shell_l, shell_nprim, shell_atom,
+                                        exps, coefs, QX_GEN_LMAX, shells, err);
+        if (rc) return nofail(rc, "%s", err.c_str());
+    }
+    const int nbf = shells.nbf;
     std::vector<PrimPair> prims;
     std::vector<PairInfo> pairs;
     std::vector<int> pcls;
-    const double kfac = std::sqrt(2.0) * std::pow(M_PI, 1.25);
-    for (int s1 = 0; s1 < nshell; ++s1)
-        for (int s2 = 0; s2 <= s1; ++s2) {
-            int f = s1, g = s2;
-            if (l[s2] > l[s1]) std::swap(f, g);
-            const double* A = coords + 3 * atom[f];
-            const double* B = coords + 3 * atom[g];
-            PairInfo pi;
-            pi.Ax = A[0]; pi.Ay = A[1]; pi.Az = A[2];
-            pi.ABx = A[0] - B[0]; pi.ABy = A[1] - B[1]; pi.ABz = A[2] - B[2];
-            const double AB2 = pi.ABx * pi.ABx + pi.ABy * pi.ABy + pi.ABz * pi.ABz;
-            pi.prim_off = (int)prims.size();
-            pi.nprim = nprim[f] * nprim[g];
-            pi.bf1 = bf[f]; pi.bf2 = bf[g];
-            pi.s1 = f; pi.s2 = g;
-            pi.atom1 = atom[f]; pi.atom2 = atom[g];
-            pi.l1 = l[f]; pi.l2 = l[g];
-            for (int p = 0; p < nprim[f]; ++p)
-                for (int q = 0; q < nprim[g]; ++q) {
-                    const double a = alpha[poff[f] + p], b = alpha[poff[g] + q];
-                    PrimPair r;
-                    r.zeta = a + b;
-                    r.oo2z = 0.5 / r.zeta;
-                    // P - A = -(b / zeta)(A - B), exactly zero for a one-centre pair (forming
-                    // P first and subtracting A leaves ~1e-15 there, which tight exponents
-                    // amplify beyond 1e-12 in integrals that vanish by symmetry)
-                    r.PAx = -(b / r.zeta) * (A[0] - B[0]);
-                    r.PAy = -(b / r.zeta) * (A[1] - B[1]);
-                    r.PAz = -(b / r.zeta) * (A[2] - B[2]);
-                    r.Px = A[0] + r.PAx; r.Py = A[1] + r.PAy; r.Pz = A[2] + r.PAz;
-                    r.K = kfac * coef[poff[f] + p] * coef[poff[g] + q] * std::exp(-a * b / r.zeta * AB2) / r.zeta;
-                    r.alpha = a;
-                    prims.push_back(r);
-                }
-            pairs.push_back(pi);
-            pcls.push_back(pair_cls(pi.l1, pi.l2));
-        }
+    build_pairs(shells, coords, prims, pairs, pcls);
     const int np = (int)pairs.size();
     // --- scratch layout part 1: Boys | prims | pairs | K per pair | diagonal lists ---
     const size_t o_prims = align256(kBoysBytes);

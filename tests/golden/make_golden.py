@@ -1,6 +1,7 @@
 """Generates tests/golden/index_golden.json from the reference's own Python helpers.
 
-Run in a container that has the reference tree: it loads quax/utils.py directly by
+Run as `python make_golden.py REFERENCE_ROOT` (or with $QUAX_REFERENCE set) where the
+reference tree is available: it loads quax/utils.py directly by
 path (that module needs only numpy and itertools; the quax package itself needs jax
 and psi4, which are absent), evaluates how_many_derivs and get_deriv_vec_idx on a
 fixed set of cases, and writes the results.  Test infrastructure only.
@@ -12,8 +13,8 @@ import sys
 
 import numpy as np
 
-REF = os.environ.get("QUAX_REFERENCE", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
+REF = None  # the reference tree: first argument, or $QUAX_REFERENCE
 
 
 def load_ref_utils():
@@ -24,6 +25,10 @@ def load_ref_utils():
 
 
 def main():
+    global REF
+    REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("QUAX_REFERENCE")
+    if not REF or not os.path.isdir(REF):
+        sys.exit("usage: make_golden.py REFERENCE_ROOT  (or set QUAX_REFERENCE)")
     ru = load_ref_utils()
     hm = [[k, n, int(ru.how_many_derivs(k, n))] for k in range(1, 7) for n in range(1, 4)]
     rng = np.random.default_rng(2024)

@@ -8,7 +8,10 @@ device array instead.  This file is collected last so that, if it fails, a run
 stopped at the first failure has already run every other test; it also passes on
 its own in a fresh process.
 
-Tolerance: 1e-12 absolute per integral, as for every FP64 ERI parity test.
+Tolerance: 1e-12 absolute per integral, as for every FP64 ERI parity test, against
+the handle path and against the CPU oracle.  The property the entry point exists
+for -- it allocates no device memory -- is checked with cudaMemGetInfo around a
+repeated call and around a call on a new basis.
 """
 import ctypes
 
@@ -45,11 +48,12 @@ def _handle_eri(basis, tol):
     return G
 
 
-def test_noalloc_matches_handle_path_two_calls():
+def test_noalloc_matches_handle_path_two_calls(oracle_lib):
     # d shells on every atom so the large (cooperative) classes take part
     spec = SyntheticSpec(natom=3, box=5.0, min_sep=1.2, kmax=3, exp_lo=0.1, exp_hi=50.0, charges=(6, 8))
     b = synthetic_molecule(spec, 11)[1]
     ref = _handle_eri(b, 1e-12)
+    oracle = torch.from_numpy(oracle_lib.compute_2e_int(oracle_lib.OracleBasis(b), 1e-12)).cuda()
     n = b.nbf()
     out = torch.full((n, n, n, n), float("nan"), dtype=torch.float64, device="cuda")
     for call in range(2):  # two calls in a row share (and reuse) the static array
@@ -57,6 +61,30 @@ def test_noalloc_matches_handle_path_two_calls():
         assert rc == 0, msg
         assert torch.isfinite(out).all()
         assert (out - ref).abs().max().item() < ATOL, f"call {call}"
+        assert (out - oracle).abs().max().item() < ATOL, f"call {call}"
+
+
+def test_noalloc_allocates_no_device_memory():
+    """After a first call (which sets the device up and lets the driver load the
+    kernels it uses), a repeated call and a call on a new basis -- the same shells
+    at displaced positions, so new tables through the same kernels -- leave the
+    device's free memory unchanged."""
+    spec = SyntheticSpec(natom=3, box=5.0, min_sep=1.2, kmax=3, exp_lo=0.1, exp_hi=50.0)
+    b1 = synthetic_molecule(spec, 2)[1]
+    b2 = b1.with_coords(b1.atom_coords() + np.random.default_rng(0).normal(0.0, 0.05, size=(b1.natom, 3)))
+    n = b1.nbf()
+    o1 = torch.empty((n, n, n, n), dtype=torch.float64, device="cuda")
+    o2 = torch.empty((n, n, n, n), dtype=torch.float64, device="cuda")
+    assert _noalloc(b1, 1e-12, o1)[0] == 0
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    assert _noalloc(b1, 1e-12, o1)[0] == 0
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert _noalloc(b2, 1e-12, o2)[0] == 0
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert (o1 - o2).abs().max().item() > 0.0  # the new basis really gave new integrals
 
 
 def test_noalloc_after_a_different_basis():
@@ -77,3 +105,21 @@ def test_noalloc_rejects_basis_beyond_the_scratch():
     out = torch.empty(1, dtype=torch.float64, device="cuda")
     rc, msg = _noalloc(big, 1e-12, out)
     assert rc == -1 and "scratch" in msg
+
+
+def test_noalloc_refuses_stream_capture():
+    """The call synchronises (it reads the Schwarz values back), so on a stream
+    that is capturing it returns an error instead of breaking the capture."""
+    b = build_basis(h2o_config1(), "sto-3g")
+    out = torch.empty((7, 7, 7, 7), dtype=torch.float64, device="cuda")
+    assert _noalloc(b, 1e-14, out)[0] == 0  # device set-up happens outside the capture
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    res = []
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s):
+            res.append(_noalloc(b, 1e-14, out))
+    rc, msg = res[0]
+    assert rc == -1 and "capturing" in msg
+    # (last in the file: a capture left open by a failure here cannot reach
+    # another test)
