@@ -231,6 +231,15 @@ int qx_engine_config(const qx_handle *h, int cls, int *cfg);
  * Synchronises the device. */
 int qx_set_engine(qx_handle *h, int cls, int plain, int pparam, int deriv, int dparam);
 
+/* Bounded waits, no counterpart in the reference: the split-mode kernels stage
+ * primitive pairs into shared memory with bulk copies and wait for them at most
+ * `polls` mbarrier polls (default 4M).  A wait that runs out sets the handle's
+ * error word (after a further bounded wait for the copies to land), which the
+ * host-synchronising calls (host outputs) report as QX_E_DEVICE and clear.  A
+ * limit of 0 makes every such wait run out: a way to exercise the failure path
+ * without faulting the GPU. */
+int qx_set_wait_limit(qx_handle *h, int polls);
+
 /* The canonical shell indices (s1, s2, s3, s4) of one class's screened unique
  * quartets, in the order of the unique layout (shells[4*qi + i], host memory of
  * 4 * nquartets ints).  No counterpart in the reference; lets a caller map the

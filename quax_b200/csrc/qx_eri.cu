@@ -265,6 +265,7 @@ struct qx_handle {
     int wpq_deriv[QX_NCLS_ALL];  // warps per quartet, derivative warp kernels
     int shard_rank = 0, shard_n = 1;
     int prim_stage = 0;  // split-mode VRR: primitive pairs staged per warp (2 x largest pair), 0 = off
+    int wait_limit = 1 << 22;  // polls of the bounded waits on those staging copies
     // J/K density screening: sqrt(K) and max |D| per pair record, threshold of the
     // call in progress (0 = off)
     double* d_kpair = nullptr;
@@ -493,6 +494,7 @@ static int run_class(qx_handle* h, int cls, int mode, const int2* d_q, long long
             QX_CUDA(cudaMemsetAsync(w.d_pacc, 0, sizeof(double) * w.nq * np, s));
             EriArgs av = a;
             av.prim_stage = h->prim_stage;
+            av.wait_limit = h->wait_limit;
             g_pvrr[cls](av, w.d_dtasks, w.ndtask, qx_der_chunk(), w.d_pacc, (int)np, s);
             wa.wpq = 1;
             wa.acc_in = w.d_pacc;
@@ -666,7 +668,8 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
     constexpr int NKEY = 64 * 64;
     const size_t nk = kept.size();
     const int nt = (int)std::max<size_t>(
-        1, std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), std::max<size_t>(1, nk / 256)));
+        1, std::min<size_t>(std::min(32u, std::max(1u, std::thread::hardware_concurrency())),
+                            std::max<size_t>(1, nk / 256)));  // <= 32: the count tables grow with the thread count
     std::vector<size_t> cut_i(nt + 1, nk);
     cut_i[0] = 0;
     for (int t = 1; t < nt; ++t) cut_i[t] = (size_t)(nk * std::sqrt((double)t / nt));
@@ -1133,6 +1136,7 @@ static int run_deriv_class(qx_handle* h, int c, int mode, double* out, const dou
                 QX_CUDA(cudaMemsetAsync(w.d_dacc, 0, sizeof(double) * a.nq * nacc, cs));
                 EriArgs av = a;
                 av.prim_stage = h->prim_stage;
+            av.wait_limit = h->wait_limit;
                 g_wvrr[c](av, tk, nt, qx_der_chunk(), w.d_dacc, (int)nacc, cs);
                 qx_launch_der_hrr(g_der_idx[c], a, mode, D, cj, ck, grad, slice, w.d_dacc, cs);
             } else if (h->deriv_eng[c] == ENG_DSPLIT) {
@@ -1140,6 +1144,7 @@ static int run_deriv_class(qx_handle* h, int c, int mode, double* out, const dou
                 QX_CUDA(cudaMemsetAsync(w.d_dacc, 0, sizeof(double) * a.nq * npad, cs));
                 EriArgs av = a;
                 av.prim_stage = h->prim_stage;
+            av.wait_limit = h->wait_limit;
                 g_dsplit[c](av, tk, nt, qx_der_chunk(), w.d_dacc, (int)npad, cs);
                 WarpArgs wa;
                 wa.e = a;
@@ -1657,6 +1662,15 @@ extern "C" int qx_set_engine(qx_handle* h, int cls, int plain, int pparam, int d
         h->deriv_eng[cls] = deriv;
         if (deriv == ENG_WARP) h->wpq_deriv[cls] = dparam;
     }
+    return QX_OK;
+}
+
+// Polls of the bounded waits on the split-mode staging copies (default 4M); a
+// wait that runs out sets the error word, which host-synchronising calls report
+// as QX_E_DEVICE.  A limit of 0 makes every such wait run out (failure-path tests).
+extern "C" int qx_set_wait_limit(qx_handle* h, int polls) {
+    if (!h || polls < 0) return fail(QX_E_INVALID, "qx_set_wait_limit: bad argument");
+    h->wait_limit = polls;
     return QX_OK;
 }
 

@@ -37,6 +37,9 @@ struct EriArgs {
     // memory with the bulk-copy (TMA) engine, bra and ket together; 0 = read them
     // from global memory
     int prim_stage = 0;
+    // polls of the bounded wait on those copies before the kernel reports a
+    // timeout through the error word
+    int wait_limit = 1 << 22;
 };
 
 // True when density screening drops this quartet from J/K.

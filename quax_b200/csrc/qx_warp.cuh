@@ -653,8 +653,11 @@ __global__ void __launch_bounds__(WARP_QPB * 32) k_gvrr(EriArgs a, const int2* _
             qx_bulk_g2s(sp, bra, bb, bar);
             qx_bulk_g2s(sp + P.nprim, ket, kb, bar);
         }
-        if (!qx_mbar_wait(bar, 0, 1 << 22)) {
+        if (!qx_mbar_wait(bar, 0, a.wait_limit)) {
+            // report the timeout, then wait (bounded) for the copies to land so
+            // none is still writing this block's shared memory when the warp exits
             if (lane == 0 && a.err) atomicOr(a.err, 1);
+            qx_mbar_wait(bar, 0, 1 << 24);
             return;
         }
         bra = sp;

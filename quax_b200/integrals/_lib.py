@@ -66,6 +66,7 @@ SIGNATURES = {
     "qx_engine_config": (C.c_int, [_vp, C.c_int, _vp]),
     "qx_set_engine": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
     "qx_class_quartets": (C.c_int, [_vp, C.c_int, _ip]),
+    "qx_set_wait_limit": (C.c_int, [_vp, C.c_int]),
     "qx_deriv_tile": (C.c_int, [_vp, C.c_int, C.c_longlong, C.c_longlong, C.c_int, _vp, C.c_longlong, _vp]),
     "qx_gamma_tile": (C.c_int, [_vp, C.c_int, C.c_longlong, C.c_longlong, C.c_int, _vp, C.c_double, C.c_double, _vp,
                                 _vp]),

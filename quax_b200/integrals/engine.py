@@ -219,6 +219,11 @@ class EriEngine:
             _lib.check(_lib.load().qx_set_engine(self.handle, int(cls), pe, int(plain_param), de, int(deriv_param)),
                        "qx_set_engine")
 
+    def set_wait_limit(self, polls: int) -> None:
+        """Polls of the bounded waits on the split-mode staging copies (0 makes
+        them run out: the host-synchronising calls then raise QuaxError)."""
+        _lib.check(_lib.load().qx_set_wait_limit(self.handle, int(polls)), "qx_set_wait_limit")
+
     def class_quartets(self, cls: int) -> np.ndarray:
         """(nq, 4) canonical shell indices of a class's quartets in list order (the
         order of the unique layout)."""

@@ -6,7 +6,7 @@ quartet counts.  Tolerance 1e-12 absolute (relative for values above 1)."""
 import numpy as np
 import pytest
 
-from quax_b200.basis import Basis, Shell
+from quax_b200.basis import Basis, Shell, SyntheticSpec, synthetic_molecule
 
 pytestmark = pytest.mark.gpu
 
@@ -49,3 +49,33 @@ def test_loose_threshold_screens_most_quartets(oracle_lib):
     tight = oracle_lib.count_unique(oracle_lib.OracleBasis(b), 1e-14)
     assert loose < tight
     _check(oracle_lib, b, 1e-4)
+
+
+def test_bounded_wait_timeout_reports_device_error(oracle_lib):
+    """Failure detection without a GPU fault: with a wait limit of 0 the split-mode
+    kernels' bounded waits on their staging copies run out, the kernels report it
+    through the error word (after letting the copies land) and return, and the
+    host call raises; with the limit restored the same handle computes the oracle's
+    tensor again (the error word was cleared)."""
+    from quax_b200.integrals import _lib
+    from quax_b200.integrals.engine import EriEngine
+
+    spec = SyntheticSpec(natom=3, box=5.0, min_sep=1.2, kmax=4, exp_lo=0.1, exp_hi=50.0, charges=(6, 8))
+    b = synthetic_molecule(spec, 3)[1]
+    eng = EriEngine(b, 1e-12)
+    forced = 0
+    for c in eng.class_info():
+        if c["nq"]:
+            try:
+                eng.set_engine(c["cls"], plain="wsplit")
+                forced += 1
+            except NotImplementedError:
+                pass
+    assert forced > 0
+    eng.set_wait_limit(0)
+    with pytest.raises(_lib.QuaxError, match="error word"):
+        eng.eri_host()
+    eng.set_wait_limit(1 << 22)
+    G = eng.eri_host().reshape(eng.nbf, eng.nbf, eng.nbf, eng.nbf)
+    ref = oracle_lib.compute_2e_int(oracle_lib.OracleBasis(b), 1e-12)
+    assert np.abs(G - ref).max() < 1e-12
