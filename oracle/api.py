@@ -64,6 +64,8 @@ def lib():
         L.qxo_quartet_blocks.argtypes = [C.POINTER(_Basis), _ip, C.c_long, _dp, C.c_int]
         L.qxo_grad_quartets.argtypes = [C.POINTER(_Basis), _ip, C.c_long, _dp, C.c_double, C.c_double, _dp,
                                         C.c_int]
+        L.qxo_shell_quartet_derivk.argtypes = [C.POINTER(_Basis), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _dp]
+        L.qxo_eri_derivk.argtypes = [C.POINTER(_Basis), C.c_double, C.c_int, C.c_long, _dp, C.c_int]
         L.qxo_how_many_derivs.argtypes = [C.c_int, C.c_int]
         L.qxo_multi_index_lookup.argtypes = [C.c_int, C.c_int, _ip]
         _LIB = L
@@ -195,6 +197,32 @@ def grad_quartets(ob: OracleBasis, shells: np.ndarray, D: np.ndarray, cj=1.0, ck
     g = np.zeros(3 * ob.natom)
     lib().qxo_grad_quartets(ob.ref, _p(q4, _ip), q4.shape[0], _p(D), float(cj), float(ck), _p(g), nthreads)
     return g
+
+
+def shell_quartet_derivk(ob: OracleBasis, s1, s2, s3, s4, k: int) -> np.ndarray:
+    """(C(11+k, k), n1, n2, n3, n4) derivative blocks of order k, all four centres
+    direct, indexed by the sorted k-tuples of centre-directions 3*centre + xyz."""
+    from math import comb
+
+    n = [(int(ob.l[s]) + 1) * (int(ob.l[s]) + 2) // 2 for s in (s1, s2, s3, s4)]
+    out = np.empty((comb(11 + k, k),) + tuple(n))
+    if lib().qxo_shell_quartet_derivk(ob.ref, s1, s2, s3, s4, int(k), _p(out)) != 0:
+        raise ValueError("derivative order must be 1..4")
+    return out
+
+
+def eri_derivk(ob: OracleBasis, thr: float, k: int, slice_idx: int = -1, nthreads: int = 0) -> np.ndarray:
+    """Order-k derivative tensor (C(3N+k-1, k), n, n, n, n), reference semantics; one
+    slice when slice_idx >= 0."""
+    from math import comb
+
+    n = ob.nbf
+    N3 = 3 * ob.natom
+    shape = (n, n, n, n) if slice_idx >= 0 else (comb(N3 + k - 1, k), n, n, n, n)
+    out = np.empty(shape)
+    if lib().qxo_eri_derivk(ob.ref, thr, int(k), int(slice_idx), _p(out), nthreads) != 0:
+        raise ValueError("derivative order must be 1..4")
+    return out
 
 
 def grad_contract(ob: OracleBasis, thr: float, D: np.ndarray, cj=1.0, ck=-0.5, nthreads: int = 0) -> np.ndarray:

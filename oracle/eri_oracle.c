@@ -1088,6 +1088,294 @@ int qxo_eri_deriv2(const qxo_basis *B, double thr, int pair_idx, double *out, in
     return 0;
 }
 
+/* ------------------------------------------------------ derivatives of order k --- */
+int qxo_multi_index_lookup(int nparams, int order, int *out);
+/* Rank of (e0, e1, e2, e3) >= 0 with sum <= K among such tuples, lexicographic. */
+static long binom_l(int n, int k) {
+    if (k < 0 || k > n) return 0;
+    long r = 1;
+    for (int i = 1; i <= k; ++i) r = r * (n - k + i) / i;
+    return r;
+}
+static int set_rank(int K, const int *e) {
+    int r = 0;
+    for (int v = 0; v < e[0]; ++v) r += (int)binom_l(K - v + 3, 3);
+    for (int v = 0; v < e[1]; ++v) r += (int)binom_l(K - e[0] - v + 2, 2);
+    for (int v = 0; v < e[2]; ++v) r += (int)binom_l(K - e[0] - e[1] - v + 1, 1);
+    return r + e[3];
+}
+
+/* Coefficients of (d/dX)^n on a 1-D Gaussian index i with unit exponent weight:
+ * d g_i = [2 alpha] g_{i+1} - i g_{i-1}; cf[j] multiplies (2 alpha)^j g_{i+2j-n}. */
+static void dexp1(int n, int i, double *cf) {
+    double c[9] = {1, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int s = 0; s < n; ++s) {
+        double nc[9] = {0};
+        for (int j = 0; j <= s; ++j) {
+            int sh = 2 * j - s;
+            nc[j + 1] += c[j];
+            nc[j] -= (double)(i + sh) * c[j];
+        }
+        memcpy(c, nc, sizeof c);
+    }
+    memcpy(cf, c, sizeof(double) * (n + 1));
+}
+
+/* All derivative blocks of order k (1..4) of the Cartesian quartet (s1 s2|s3 s4),
+ * every centre differentiated directly (no translational invariance):
+ * out[m * nblk + o], m = rank of the sorted k-tuple of centre-directions
+ * (3 * centre + xyz) among all such tuples over 12 values (Libint's order of
+ * derivative buffers), o = block element.  Obara-Saika VRR of [e0|f0] raised by k
+ * on each side, accumulated over primitives in weighted sets
+ * (2a)^eA (2b)^eB (2c)^eC (2d)^eD, sum e <= k; the derivative identity applied
+ * per centre and direction picks the set and the shifted block (HRR cached). */
+static int quartetk(const qxo_basis *B, int s1, int s2, int s3, int s4, int k, double *out) {
+    if (k < 1 || k > 4) return -1;
+    int L[4] = {B->l[s1], B->l[s2], B->l[s3], B->l[s4]};
+    int sh[4] = {s1, s2, s3, s4};
+    const double *Cn[4];
+    for (int c = 0; c < 4; ++c) Cn[c] = B->center + 3 * sh[c];
+    double AB[3], CD[3];
+    for (int i = 0; i < 3; ++i) { AB[i] = Cn[0][i] - Cn[1][i]; CD[i] = Cn[2][i] - Cn[3][i]; }
+    double AB2 = AB[0] * AB[0] + AB[1] * AB[1] + AB[2] * AB[2];
+    double CD2 = CD[0] * CD[0] + CD[1] * CD[1] + CD[2] * CD[2];
+    int E = L[0] + L[1] + k, F = L[2] + L[3] + k;
+    int NE = hoff(E + 1), NF = hoff(F + 1), M = E + F + 1;
+    size_t vsz = (size_t)NE * NF * M, asz = (size_t)NE * NF;
+    int NS = (int)binom_l(k + 4, 4);
+    double *v = (double *)malloc(sizeof(double) * (vsz + NS * asz));
+    double *S = v + vsz;
+    memset(S, 0, sizeof(double) * NS * asz);
+    int sets[70][4], ns = 0;
+    for (int a = 0; a <= k; ++a)
+        for (int b = 0; a + b <= k; ++b)
+            for (int c = 0; a + b + c <= k; ++c)
+                for (int d = 0; a + b + c + d <= k; ++d) {
+                    sets[ns][0] = a; sets[ns][1] = b; sets[ns][2] = c; sets[ns][3] = d;
+                    ++ns;
+                }
+    double Fm[4 * QXO_LMAX + 8];
+    const double pref0 = 2.0 * pow(M_PI, 2.5);
+    for (int p1 = 0; p1 < B->nprim[s1]; ++p1)
+        for (int p2 = 0; p2 < B->nprim[s2]; ++p2) {
+            double a = B->alpha[B->prim_off[s1] + p1], b = B->alpha[B->prim_off[s2] + p2];
+            double zeta = a + b, P[3], PA[3];
+            for (int i = 0; i < 3; ++i) { PA[i] = -(b / zeta) * AB[i]; P[i] = Cn[0][i] + PA[i]; }
+            double Kab = exp(-a * b / zeta * AB2) * B->coef[B->prim_off[s1] + p1] * B->coef[B->prim_off[s2] + p2];
+            for (int p3 = 0; p3 < B->nprim[s3]; ++p3)
+                for (int p4 = 0; p4 < B->nprim[s4]; ++p4) {
+                    double c = B->alpha[B->prim_off[s3] + p3], d = B->alpha[B->prim_off[s4] + p4];
+                    double eta = c + d, Q[3], QC[3], WP[3], WQ[3], PQ2 = 0.0;
+                    for (int i = 0; i < 3; ++i) { QC[i] = -(d / eta) * CD[i]; Q[i] = Cn[2][i] + QC[i]; }
+                    double Kcd = exp(-c * d / eta * CD2) * B->coef[B->prim_off[s3] + p3] * B->coef[B->prim_off[s4] + p4];
+                    double rho = zeta * eta / (zeta + eta);
+                    for (int i = 0; i < 3; ++i) {
+                        double PQ = (Cn[0][i] - Cn[2][i]) + PA[i] - QC[i];
+                        WP[i] = -eta / (zeta + eta) * PQ;
+                        WQ[i] = zeta / (zeta + eta) * PQ;
+                        PQ2 += PQ * PQ;
+                    }
+                    (void)P; (void)Q;
+                    qxo_boys(E + F, rho * PQ2, Fm);
+                    vrr(E, F, zeta, eta, PA, WP, QC, WQ, rho, Fm, pref0 / (zeta * eta * sqrt(zeta + eta)) * Kab * Kcd, v);
+                    double e2[4] = {2 * a, 2 * b, 2 * c, 2 * d};
+                    for (int q = 0; q < ns; ++q) {
+                        double w = 1.0;
+                        for (int cc = 0; cc < 4; ++cc)
+                            for (int t = 0; t < sets[q][cc]; ++t) w *= e2[cc];
+                        double *Sq = S + (size_t)set_rank(k, sets[q]) * asz;
+                        for (size_t h = 0; h < (size_t)NE; ++h)
+                            for (int g = 0; g < NF; ++g) Sq[h * NF + g] += w * v[(h * NF + g) * M];
+                    }
+                }
+        }
+    int n[4];
+    for (int c = 0; c < 4; ++c) n[c] = ncart(L[c]);
+    size_t nblk = (size_t)n[0] * n[1] * n[2] * n[3];
+    /* HRR blocks cached by (set, shifts in [-k, k] per centre) */
+    const int W = 2 * k + 1;
+    size_t ncache = (size_t)NS * W * W * W * W;
+    double **cache = (double **)calloc(ncache, sizeof(double *));
+    int nm = (int)binom_l(11 + k, k);
+    int tup[4] = {0, 0, 0, 0};
+    for (int m = 0; m < nm; ++m) {
+        /* per centre and direction: derivative count */
+        int cnt[4][3];
+        memset(cnt, 0, sizeof cnt);
+        for (int i = 0; i < k; ++i) cnt[tup[i] / 3][tup[i] % 3]++;
+        double *dst = out + (size_t)m * nblk;
+        for (int ia = 0; ia < n[0]; ++ia)
+            for (int ib = 0; ib < n[1]; ++ib)
+                for (int ic = 0; ic < n[2]; ++ic)
+                    for (int id = 0; id < n[3]; ++id) {
+                        const int *xs[4] = {g_comp[L[0]][ia], g_comp[L[1]][ib], g_comp[L[2]][ic], g_comp[L[3]][id]};
+                        /* expansion coefficients per (centre, direction) */
+                        double cf[4][3][5];
+                        int nt[4][3];
+                        for (int cc = 0; cc < 4; ++cc)
+                            for (int x = 0; x < 3; ++x) {
+                                dexp1(cnt[cc][x], xs[cc][x], cf[cc][x]);
+                                nt[cc][x] = cnt[cc][x] + 1;
+                            }
+                        double val = 0.0;
+                        /* iterate over all 12 term indices (mixed radix) */
+                        int j[12] = {0};
+                        for (;;) {
+                            double coef = 1.0;
+                            int comp[4][3], raise[4] = {0, 0, 0, 0}, ok = 1;
+                            for (int cc = 0; cc < 4 && ok; ++cc)
+                                for (int x = 0; x < 3; ++x) {
+                                    int jj = j[3 * cc + x];
+                                    coef *= cf[cc][x][jj];
+                                    comp[cc][x] = xs[cc][x] + 2 * jj - cnt[cc][x];
+                                    raise[cc] += jj;
+                                    if (comp[cc][x] < 0) ok = 0;
+                                }
+                            if (ok && coef != 0.0) {
+                                int dl[4];
+                                for (int cc = 0; cc < 4; ++cc) dl[cc] = comp[cc][0] + comp[cc][1] + comp[cc][2] - L[cc];
+                                int srank = set_rank(k, raise);
+                                size_t key = ((((size_t)srank * W + dl[0] + k) * W + dl[1] + k) * W + dl[2] + k) * W + dl[3] + k;
+                                if (!cache[key]) {
+                                    size_t bs = (size_t)ncart(L[0] + dl[0]) * ncart(L[1] + dl[1]) * ncart(L[2] + dl[2]) *
+                                                ncart(L[3] + dl[3]);
+                                    cache[key] = (double *)malloc(sizeof(double) * bs);
+                                    hrr_both(L[0] + dl[0], L[1] + dl[1], L[2] + dl[2], L[3] + dl[3], AB, CD,
+                                             S + (size_t)srank * asz, NF, cache[key]);
+                                }
+                                int nb2 = ncart(L[1] + dl[1]), nc2 = ncart(L[2] + dl[2]), nd2 = ncart(L[3] + dl[3]);
+                                size_t o = (((size_t)lidx(comp[0][0], comp[0][1], comp[0][2]) * nb2 +
+                                             lidx(comp[1][0], comp[1][1], comp[1][2])) * nc2 +
+                                            lidx(comp[2][0], comp[2][1], comp[2][2])) * nd2 +
+                                           lidx(comp[3][0], comp[3][1], comp[3][2]);
+                                val += coef * cache[key][o];
+                            }
+                            int p = 0;
+                            while (p < 12) {
+                                if (++j[p] < nt[p / 3][p % 3]) break;
+                                j[p] = 0;
+                                ++p;
+                            }
+                            if (p == 12) break;
+                        }
+                        dst[(((size_t)ia * n[1] + ib) * n[2] + ic) * n[3] + id] = val;
+                    }
+        /* next sorted tuple */
+        int p = k - 1;
+        while (p >= 0 && tup[p] == 11) --p;
+        if (p < 0) break;
+        tup[p] += 1;
+        for (int i = p + 1; i < k; ++i) tup[i] = tup[p];
+    }
+    for (size_t i = 0; i < ncache; ++i) free(cache[i]);
+    free(cache);
+    free(v);
+    return 0;
+}
+
+int qxo_shell_quartet_derivk(const qxo_basis *B, int s1, int s2, int s3, int s4, int k, double *out) {
+    init_tables();
+    return quartetk(B, s1, s2, s3, s4, k, out);
+}
+
+/* Derivative tensor of order k (1..4) with the reference's semantics
+ * (eri_deriv_core, libint_interface.cc:2582-2779, and compute_2e_deriv, :1097-1335):
+ * slices for the sorted nuclear multi-indices nu_1 <= ... <= nu_k in the order of
+ * generate_multi_index_lookup(3N, k); element = sum over the cartesian product of
+ * shell positions on each nu_i's atom (direction of nu_i) of the buffer of the
+ * sorted centre-direction tuple (libint_interface.cc:1200-1226).  Quartets on one
+ * atom are skipped.  slice >= 0 produces that slice only. */
+int qxo_eri_derivk(const qxo_basis *B, double thr, int k, long slice, double *out, int nthreads) {
+    init_tables();
+    if (k < 1 || k > 4) return -1;
+    int ns = B->nshell, N3 = 3 * B->natom;
+    double *K = (double *)malloc(sizeof(double) * ns * ns);
+    double kmax;
+    qxo_schwarz(B, K, &kmax, nthreads);
+    int *pairs = (int *)malloc(sizeof(int) * ns * (ns + 1));
+    int np = qxo_pairs(B, K, kmax, thr, pairs);
+    long *s2bf = (long *)malloc(sizeof(long) * ns);
+    long n;
+    shell2bf_of(B, s2bf, &n);
+    size_t n4 = (size_t)n * n * n * n;
+    long nslot = binom_l(N3 + k - 1, k);
+    long nslice = slice >= 0 ? 1 : nslot;
+    memset(out, 0, sizeof(double) * n4 * nslice);
+    int *nus = (int *)malloc(sizeof(int) * nslot * k);
+    qxo_multi_index_lookup(N3, k, nus);
+    int nm = (int)binom_l(11 + k, k);
+    double thr2 = thr * thr;
+    int lmx = 0;
+    for (int s = 0; s < ns; ++s) lmx = B->l[s] > lmx ? B->l[s] : lmx;
+    size_t nbmax = (size_t)ncart(lmx) * ncart(lmx) * ncart(lmx) * ncart(lmx);
+    int nt = nthreads_of(nthreads);
+#pragma omp parallel num_threads(nt)
+    {
+        double *buf = (double *)malloc(sizeof(double) * nbmax * nm);
+#pragma omp for schedule(dynamic)
+        for (int ip = 0; ip < np; ++ip) {
+            int p1 = pairs[2 * ip], p2 = pairs[2 * ip + 1];
+            for (int jp = 0; jp < np; ++jp) {
+                int p3 = pairs[2 * jp], p4 = pairs[2 * jp + 1];
+                if (K[p1 * ns + p2] * K[p3 * ns + p4] < thr2) continue;
+                int at[4] = {B->atom[p1], B->atom[p2], B->atom[p3], B->atom[p4]};
+                if (at[0] == at[1] && at[0] == at[2] && at[0] == at[3]) continue;
+                quartetk(B, p1, p2, p3, p4, k, buf);
+                int nn[4] = {shell_size(B->l[p1]), shell_size(B->l[p2]), shell_size(B->l[p3]), shell_size(B->l[p4])};
+                size_t nblk = (size_t)nn[0] * nn[1] * nn[2] * nn[3];
+                long b1 = s2bf[p1], b2 = s2bf[p2], b3 = s2bf[p3], b4 = s2bf[p4];
+                for (long sl = 0; sl < nslice; ++sl) {
+                    long r = slice >= 0 ? slice : sl;
+                    const int *nu = nus + r * k;
+                    /* choices per derivative operator: positions on its atom */
+                    int choice[4][4], nch[4], ok = 1;
+                    for (int i = 0; i < k; ++i) {
+                        nch[i] = 0;
+                        for (int c = 0; c < 4; ++c)
+                            if (at[c] == nu[i] / 3) choice[i][nch[i]++] = 3 * c + nu[i] % 3;
+                        if (!nch[i]) ok = 0;
+                    }
+                    if (!ok) continue;
+                    /* buffer indices of the cartesian product (sorted) */
+                    int bidx[256], nb = 0, pick[4] = {0, 0, 0, 0};
+                    for (;;) {
+                        int tpl[4];
+                        for (int i = 0; i < k; ++i) tpl[i] = choice[i][pick[i]];
+                        for (int i = 1; i < k; ++i)
+                            for (int q = i; q > 0 && tpl[q - 1] > tpl[q]; --q) { int t = tpl[q]; tpl[q] = tpl[q - 1]; tpl[q - 1] = t; }
+                        long rk = 0;
+                        int prev = 0;
+                        for (int i = 0; i < k; ++i) {
+                            for (int x = prev; x < tpl[i]; ++x) rk += binom_l(12 - x + k - i - 2, k - i - 1);
+                            prev = tpl[i];
+                        }
+                        bidx[nb++] = (int)rk;
+                        int q = k - 1;
+                        while (q >= 0 && ++pick[q] == nch[q]) { pick[q] = 0; --q; }
+                        if (q < 0) break;
+                    }
+                    double *o = out + (size_t)sl * n4;
+                    for (int f1 = 0, idx = 0; f1 < nn[0]; ++f1)
+                        for (int f2 = 0; f2 < nn[1]; ++f2)
+                            for (int f3 = 0; f3 < nn[2]; ++f3)
+                                for (int f4 = 0; f4 < nn[3]; ++f4, ++idx) {
+                                    double x = 0.0;
+                                    for (int t = 0; t < nb; ++t) x += buf[(size_t)bidx[t] * nblk + idx];
+                                    long i = b1 + f1, j = b2 + f2, kk = b3 + f3, l = b4 + f4;
+                                    o[((i * n + j) * n + kk) * n + l] += x;
+                                    if (p1 != p2) o[((j * n + i) * n + kk) * n + l] += x;
+                                    if (p3 != p4) o[((i * n + j) * n + l) * n + kk] += x;
+                                    if (p1 != p2 && p3 != p4) o[((j * n + i) * n + l) * n + kk] += x;
+                                }
+                }
+            }
+        }
+        free(buf);
+    }
+    free(K); free(pairs); free(s2bf); free(nus);
+    return 0;
+}
+
 /* Index helpers restated from quax/integrals/utils.h:131-172. */
 int qxo_how_many_derivs(int k, int n) {
     long val = 1, fact = 1;

@@ -109,12 +109,16 @@ struct RysCls {
     // team size: about 12 components per thread (8 for the gradient tile, which
     // keeps 9 sums per component), 32..256 threads
     static constexpr int TS0 = KIND == RK_GRADT ? (NCOMP + 7) / 8 : (NCOMP + 11) / 12;
-    static constexpr int TS = TS0 <= 32 ? 32 : TS0 <= 64 ? 64 : TS0 <= 128 ? 128 : 256;
+    static constexpr int TS1 = TS0 <= 32 ? 32 : TS0 <= 64 ? 64 : TS0 <= 128 ? 128 : 256;
+    static constexpr int HDR = RYS_HDR + (KIND >= RK_DER1 ? RYS_DERK_HDR : 0);
+    static constexpr int PER_ROOT = 3 * (USZ + UOPS);
+    // one root per batch with (128 / TS1) teams per block must fit; otherwise the
+    // block holds a single team of 128 threads (the large derivative kinds)
+    static constexpr bool MULTI = TS1 >= 128 || (128 / TS1) * (HDR + PER_ROOT) * 8 <= RYS_SMEM_MAX;
+    static constexpr int TS = MULTI ? TS1 : 128;
     static constexpr int BS = TS < 128 ? 128 : TS;
     static constexpr int TPB = BS / TS;
     static constexpr int NCPT = (NCOMP + TS - 1) / TS;
-    static constexpr int HDR = RYS_HDR + (KIND >= RK_DER1 ? RYS_DERK_HDR : 0);
-    static constexpr int PER_ROOT = 3 * (USZ + UOPS);
     static constexpr int RB0 = (RYS_SMEM_TARGET / 8 / TPB - HDR) / PER_ROOT;
     static constexpr int RB = RB0 < 1 ? 1 : (RB0 > NR ? NR : RB0);
     static constexpr int TEAM_SMEM = HDR + RB * PER_ROOT;  // doubles

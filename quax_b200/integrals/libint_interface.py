@@ -230,3 +230,8 @@ def eri_deriv_core_device(deriv_order: int = 1):
 def engine() -> EriEngine:
     """The engine behind the module state (for the adjoint gradient and friends)."""
     return _engine()
+
+
+def is_initialized() -> bool:
+    """True between initialize() and finalize()."""
+    return _state.get("engine") is not None

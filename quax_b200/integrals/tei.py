@@ -4,42 +4,88 @@ The reference (quax/integrals/tei.py:12-181, 336-346, 403-411) defines JAX
 primitives ``eri`` and ``eri_deriv`` whose JVP treats the incoming tangent as an
 integer derivative-order vector (valid for the one-hot tangents jacfwd feeds),
 plus a batching rule that loops over the one-hot rows.  JAX is not installed on
-this image, so the same rules are given here as plain methods on torch tensors:
+this image, so the same rules are given here as plain methods on torch tensors,
+with the reference's signatures:
 
+    TEI(basis1, basis2, basis3, basis4, xyz_path, max_deriv_order, options, mode)
+                                    (tei.py:14; basis objects with .nbf() or basis
+                                    names; the geometry read from xyz_path)
     eri(geom)                       -> (n,n,n,n) device tensor
-    eri_deriv(geom, deriv_vec)      -> (n,n,n,n) slice, mode 'core' (precomputed
-                                       first-derivative tensor, tei.py:31-34) or
-                                       'f12' (computed per call, tei.py:152-154)
+    eri_deriv(geom, deriv_vec)      -> (n,n,n,n) slice: mode 'core' (precomputed
+                                       tensors of every order <= max_deriv_order,
+                                       tei.py:29-34), 'f12' (computed per call,
+                                       tei.py:152-154) or 'disk' (eri_derivs, else
+                                       eri_partials, tei.py:157-181)
     eri_jvp((geom,), (tangent,))    -> (eri, eri_deriv(geom, tangent)) (tei.py:336-340)
     eri_deriv_jvp(...)              -> deriv_vec + tangent selects the next order
-    eri_deriv_batch(geom, rows)     -> stacked slices for a batch of one-hot rows
+    eri_deriv_batch(batched_args, batch_dims)
+                                    -> (stacked slices of the one-hot rows, 0)
+                                       (tei.py:403-411)
 
-``geom`` is a placeholder exactly as in the reference: the integrals are evaluated
-at the geometry the engine was built with.  The differentiable entry point that
-does use the geometry is :class:`EriEnergy` / :func:`two_electron_gradient`,
-which contract the adjoint kernel instead of materialising 3N x n^4 tensors.
+Like the reference, the integrals come from the ``libint_interface`` module's
+state (set by its initialize(), quax/methods/ints.py:20): a TEI built while that
+module is initialised uses its engine.  Otherwise the TEI initialises it from
+xyz_path and the basis (a name, or an in-memory Basis whose shells sit on the
+xyz file's atoms).  ``geom`` is a placeholder exactly as in the reference: the
+integrals are evaluated at the geometry the engine was built with.  The
+differentiable entry point that does use the geometry is
+:func:`two_electron_energy`, whose backward pass is the adjoint kernel.
 """
 from __future__ import annotations
+
+import os
 
 import numpy as np
 import torch
 
+from ..basis import Basis, Molecule
 from ..utils import get_deriv_vec_idx, how_many_derivs
 from . import _lib
 from .engine import EriEngine
 
 
+def _nbf(basis) -> int:
+    """nbf() of a basis object (the reference passes psi4 BasisSet objects)."""
+    return int(basis.nbf()) if callable(getattr(basis, "nbf", None)) else int(basis.nbf)
+
+
 class TEI:
-    def __init__(self, basis, max_deriv_order: int = 0, mode: str = "core", ints_tol: float = 1.0e-14,
-                 engine: EriEngine | None = None):
-        self.engine = engine if engine is not None else EriEngine(basis, ints_tol)
-        self.natom = self.engine.natom
-        self.nbf = self.engine.nbf
-        self.mode = mode
-        # mode "disk" (tei.py:157-181): derivative slices are read from
-        # eri_derivs.(h5|npz) written by libint_interface.compute_2e_deriv_disk
+    def __init__(self, basis1, basis2=None, basis3=None, basis4=None, xyz_path=None, max_deriv_order: int = 0,
+                 options=None, mode: str = "core", *, ints_tol: float | None = None, engine: EriEngine | None = None):
+        from . import libint_interface as li
+
+        options = dict(options or {})
+        tol = ints_tol if ints_tol is not None else float(options.get("ints_tolerance", 1.0e-14))
         if mode not in ("core", "f12", "disk"):
             raise ValueError(f"unknown mode {mode}")
+        if engine is None:
+            if xyz_path is not None:
+                # the reference's form: natoms from the xyz file, nbf from the bases
+                mol = Molecule.from_xyz(xyz_path, units="angstrom")
+                bases = [b for b in (basis1, basis2, basis3, basis4) if b is not None]
+                if len({_nbf(b) if not isinstance(b, str) else b for b in bases}) > 1:
+                    raise NotImplementedError("the ERI path uses one basis for all four centres")
+                if li.is_initialized():
+                    engine = li.engine()
+                elif isinstance(basis1, str):
+                    li.initialize(xyz_path, basis1, basis1, basis1, basis1, tol)
+                    engine = li.engine()
+                else:
+                    li.initialize_basis(basis1.with_coords(mol.coords), tol, charges=mol.Z)
+                    engine = li.engine()
+                if engine.natom != mol.natom:
+                    raise ValueError(f"{xyz_path} has {mol.natom} atoms, the integral engine {engine.natom}")
+            else:
+                # in-memory basis (this package's own callers)
+                if not isinstance(basis1, Basis):
+                    raise ValueError("TEI needs xyz_path, or an in-memory Basis as basis1")
+                engine = EriEngine(basis1, tol)
+        self.engine = engine
+        self.natom = engine.natom
+        self.nbf = self.nbf1 = self.nbf2 = self.nbf3 = self.nbf4 = engine.nbf
+        if basis1 is not None and not isinstance(basis1, str) and _nbf(basis1) != self.nbf:
+            raise ValueError(f"basis has {_nbf(basis1)} functions, the integral engine {self.nbf}")
+        self.mode = mode
         self.eri_derivatives = []
         if mode == "core" and max_deriv_order > 0:
             # tei.py:29-34: one tensor of unique derivatives per order
@@ -64,12 +110,28 @@ class TEI:
                 raise NotImplementedError(f"order {order} derivatives were not precomputed")
             return self.eri_derivatives[order - 1][get_deriv_vec_idx(dv)]
         if self.mode == "disk":
-            from .libint_interface import read_dataset
-
-            n = self.nbf
-            data = read_dataset("eri_derivs", f"eri_{n}_{n}_{n}_{n}_deriv{order}")
-            return torch.from_numpy(np.ascontiguousarray(data[..., get_deriv_vec_idx(dv)])).to(self.engine.device)
+            return self._read_disk(order, get_deriv_vec_idx(dv))
         return self.engine.eri_deriv(dv)
+
+    def _read_disk(self, order: int, idx: int) -> torch.Tensor:
+        """tei.py:157-181: the full tensors eri_derivs (datasets eri_n_n_n_n_deriv<k>,
+        derivative index last), else the per-slice file eri_partials (datasets
+        eri_n_n_n_n_deriv<k>_<idx>); .h5 where h5py is present, .npz otherwise."""
+        from .libint_interface import read_dataset
+
+        n = self.nbf
+        base = f"eri_{n}_{n}_{n}_{n}_deriv{order}"
+        if os.path.exists("eri_derivs.h5") or os.path.exists("eri_derivs.npz"):
+            data = read_dataset("eri_derivs", base)
+        elif os.path.exists("eri_partials.h5") or os.path.exists("eri_partials.npz"):
+            data = read_dataset("eri_partials", f"{base}_{idx}")
+        else:
+            raise FileNotFoundError("ERI derivatives not found on disk")
+        if data.ndim == 5:
+            data = data[..., idx]
+        elif data.ndim != 4:
+            raise ValueError("Something went wrong reading integral derivative file")
+        return torch.from_numpy(np.ascontiguousarray(data)).to(self.engine.device)
 
     def eri_jvp(self, primals, tangents):
         (geom,) = primals
@@ -80,8 +142,11 @@ class TEI:
         dv = np.asarray(deriv_vec, dtype=int) + np.asarray(tangents[0], dtype=int)
         return self.eri_deriv(geom, deriv_vec), self.eri_deriv(geom, dv)
 
-    def eri_deriv_batch(self, geom, deriv_batch):
-        return torch.stack([self.eri_deriv(geom, row) for row in deriv_batch]), 0
+    def eri_deriv_batch(self, batched_args, batch_dims):
+        """tei.py:403-411: evaluate every row of the batched deriv_vec argument and
+        stack the slices along a new leading axis, which is the output batch axis."""
+        geom_batch, deriv_batch = batched_args
+        return torch.stack([self.eri_deriv(geom_batch, row) for row in deriv_batch]), 0
 
 
 class _EriEnergy(torch.autograd.Function):

@@ -56,9 +56,49 @@ def test_tei_jvp_and_batch_semantics():
     G, dG = core.eri_jvp((geom,), (rows[4],))
     assert torch.equal(G, core.eri(geom))
     assert (dG - f12.eri_deriv(geom, rows[4])).abs().max().item() < 1e-12
-    batch, axis = core.eri_deriv_batch(geom, rows)
+    batch, axis = core.eri_deriv_batch((geom, rows), (None, 0))  # tei.py:403-411's signature
     assert axis == 0 and batch.shape == (9, 7, 7, 7, 7)
     assert (batch - core.eri_derivatives[0]).abs().max().item() == 0.0
+
+
+def test_tei_reference_constructor(tmp_path, oracle_lib):
+    """TEI(basis1, basis2, basis3, basis4, xyz_path, max_deriv_order, options, mode)
+    as quax/methods/ints.py builds it: libint_interface initialised from the xyz
+    file first, then the TEI on the module's state; slices equal the oracle's."""
+    from quax_b200.basis import Molecule
+    from quax_b200.integrals import libint_interface as li
+    from quax_b200.integrals.tei import TEI
+
+    mol = h2o_config1()
+    xyz = str(tmp_path / "h2o.xyz")
+    mol.to_xyz(xyz)
+    b = build_basis(Molecule.from_xyz(xyz, units="angstrom"), "sto-3g")
+    ob = oracle_lib.OracleBasis(b)
+    li.initialize(xyz, "sto-3g", "sto-3g", "sto-3g", "sto-3g", 1e-14)
+    try:
+        tei = TEI(b, b, b, b, xyz, 2, {"ints_tolerance": 1e-14}, "core")
+        assert tei.engine is li.engine() and tei.nbf1 == 7
+        dv = np.zeros(9, dtype=int)
+        dv[4] = 1
+        ref = oracle_lib.eri_deriv1(ob, 1e-14, deriv_idx=4)
+        assert np.abs(tei.eri_deriv(torch.zeros(9), dv).cpu().numpy() - ref).max() < 1e-11
+        dv[7] = 1
+        from quax_b200.utils import get_deriv_vec_idx
+
+        ref2 = oracle_lib.eri_deriv2(ob, 1e-14, pair_idx=get_deriv_vec_idx(dv))
+        assert np.abs(tei.eri_deriv(torch.zeros(9), dv).cpu().numpy() - ref2).max() < 1e-11
+        assert np.abs(tei.eri(torch.zeros(9)).cpu().numpy() - oracle_lib.compute_2e_int(ob, 1e-14)).max() < 1e-12
+    finally:
+        li.finalize()
+    # without an initialised module the TEI initialises it from the xyz file and basis name
+    tei = TEI("sto-3g", "sto-3g", "sto-3g", "sto-3g", xyz, 0, {}, "f12")
+    try:
+        dv = np.zeros(9, dtype=int)
+        dv[2] = 1
+        ref = oracle_lib.eri_deriv1(ob, 1e-14, deriv_idx=2)
+        assert np.abs(tei.eri_deriv(None, dv).cpu().numpy() - ref).max() < 1e-11
+    finally:
+        li.finalize()
 
 
 def test_adjoint_autograd_against_finite_differences():
@@ -119,5 +159,14 @@ def test_disk_mode_roundtrip(tmp_path, monkeypatch):
         s1 = li.read_dataset("oei_derivs", f"overlap_{n}_{n}_deriv1")
         assert s1.shape == (n, n, 9)
         assert path.startswith("eri_derivs.")
+        # without eri_derivs the per-slice file eri_partials is read (tei.py:164-168):
+        # datasets eri_n_n_n_n_deriv<k>_<flattened index>, four-dimensional
+        os.remove(path)
+        idx = get_deriv_vec_idx(dv)
+        np.savez("eri_partials.npz", **{f"eri_{n}_{n}_{n}_{n}_deriv2_{idx}": d2[..., idx]})
+        assert np.abs(tei.eri_deriv(None, dv).cpu().numpy() - d2[..., idx]).max() == 0.0
+        os.remove("eri_partials.npz")
+        with pytest.raises(FileNotFoundError):
+            tei.eri_deriv(None, dv)
     finally:
         li.finalize()

@@ -22,6 +22,7 @@ ATOL = 1e-12
 ATOL_DF = 1e-9  # derivative tensors with f shells
 ATOL_D = 1e-11  # derivative tensors with d shells
 ATOL_G = 1e-9
+HIGH_ORDER_TOL = {3: 5e-8, 4: 1e-6}  # order-3/4 tensors: the oracle's error (see the tests)
 
 
 def _engine(basis, tol):
@@ -204,3 +205,46 @@ def test_plain_tiled_gradient_equals_adjoint(oracle_lib, images):
     scale = max(1.0, np.abs(gr).max())
     assert np.abs(gp - ga).max() < ATOL_G * scale
     assert np.abs(gp - gr).max() < ATOL_G * scale
+
+
+@pytest.mark.parametrize("k", [3, 4])
+def test_h2o_high_order_deriv_core(oracle_lib, k):
+    """Orders 3 and 4 (the reference reaches them by nested jacfwd,
+    quax/core.py:93-97): the dense tensor (C(3N+k-1, k), n, n, n, n) and one slice
+    against the oracle's order-k tensor with the reference's cartesian-product
+    semantics.  Tolerance HIGH_ORDER_TOL[k] x max(1, max |value|), set by the
+    oracle's own error: against 40-digit values of the worst elements, the oracle
+    is off by 3.1e-10 (order 3) and 3.3e-7 (order 4), the GPU by 1.0e-11 and 4.1e-9
+    (an order-k derivative carries factors up to (2 alpha)^k, alpha = 130.7 for the
+    oxygen 1s here)."""
+    from quax_b200.basis import build_basis, h2o_config1
+    from quax_b200.utils import get_deriv_vec_idx
+
+    b = build_basis(h2o_config1(), "sto-3g")
+    eng = _engine(b, 1e-14)
+    ob = oracle_lib.OracleBasis(b)
+    d = eng.eri_deriv_core(k).cpu().numpy()
+    ref = oracle_lib.eri_derivk(ob, 1e-14, k)
+    scale = max(1.0, np.abs(ref).max())
+    assert d.shape == ref.shape
+    err = np.abs(d - ref).max()
+    assert err < HIGH_ORDER_TOL[k] * scale, err
+    dv = np.zeros(9, dtype=int)
+    dv[1] += 1
+    dv[4] += k - 2
+    dv[8] += 1
+    s = eng.eri_deriv(dv).cpu().numpy()
+    assert np.abs(s - ref[get_deriv_vec_idx(dv)]).max() < HIGH_ORDER_TOL[k] * scale
+
+
+def test_order3_with_d_shells(oracle_lib):
+    """Order 3 with d shells (every l <= 2 class has an order-3 program); the
+    worst element's oracle error is 1.2e-8 against its 40-digit value (GPU 3.4e-9)."""
+    spec = SyntheticSpec(natom=2, box=3.0, min_sep=1.2, kmax=2, exp_lo=0.2, exp_hi=20.0, heavy_ls=(0, 1, 2),
+                         h_ls=(0, 1))
+    b = synthetic_molecule(spec, 6)[1]
+    eng = _engine(b, 1e-12)
+    d = eng.eri_deriv_core(3).cpu().numpy()
+    ref = oracle_lib.eri_derivk(oracle_lib.OracleBasis(b), 1e-12, 3)
+    err = np.abs(d - ref).max()
+    assert err < HIGH_ORDER_TOL[3] * max(1.0, np.abs(ref).max()), err
