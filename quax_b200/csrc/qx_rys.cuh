@@ -71,12 +71,12 @@ struct RysKind<RK_PLAIN> {
     static constexpr int ORD = 0, KA = 0, KB = 0, KC = 0, KD = 0, NOPS = 0;
 };
 template <>
-struct RysKind<RK_GRAD> {  // A, B, C raised by one; tables I, dA, dB, dC (D by invariance)
-    static constexpr int ORD = 1, KA = 1, KB = 1, KC = 1, KD = 0, NOPS = 4;
+struct RysKind<RK_GRAD> {  // A, B, C raised by one; dA, dB, dC formed in the products (D by invariance)
+    static constexpr int ORD = 1, KA = 1, KB = 1, KC = 1, KD = 0, NOPS = 0;
 };
 template <>
 struct RysKind<RK_GRADT> {  // as RK_GRAD, but the 9 derivative integrals are written to a tile
-    static constexpr int ORD = 1, KA = 1, KB = 1, KC = 1, KD = 0, NOPS = 4;
+    static constexpr int ORD = 1, KA = 1, KB = 1, KC = 1, KD = 0, NOPS = 0;
 };
 template <>
 struct RysKind<RK_HVP> {  // A, B, C raised by two; tables I, dA, dB, dC, V, dA V, dB V, dC V
@@ -125,7 +125,13 @@ struct RysCls {
     static constexpr int SMEM = TPB * TEAM_SMEM * 8;       // bytes per block
     static constexpr bool FITS = SMEM <= RYS_SMEM_MAX;
     // offsets of one component in a table are packed 10 bits per direction
-    static_assert((KIND != RK_PLAIN || SRAW < 1024) && SZ0 < 1024, "1-D table offsets exceed 10 bits");
+    // products read the raw transferred table (plain and gradient kinds) or the
+    // op tables (the others)
+    static constexpr bool RAW = KIND == RK_PLAIN || KIND == RK_GRAD || KIND == RK_GRADT;
+    static_assert((!RAW || SRAW < 1024) && SZ0 < 1024, "1-D table offsets exceed 10 bits");
+    // one thread builds a whole (direction, root) unit -- 2-D table and both
+    // transfers -- when the units keep at least a sixth of the team busy or are small
+    static constexpr bool SEQ = 6 * RB >= TS || SRAW <= 160;
     // derivative tensors: multi-indices accumulated per pass over the primitives
     static constexpr int MG = NCPT >= 32 ? 1 : (32 / NCPT > 8 ? 8 : 32 / NCPT);
     // gradient tile: derivative coordinates (of the 9) accumulated per pass
@@ -342,6 +348,50 @@ QX_HD inline void rys_phase_ket(const RysPrim& s, int d, int nrb, double* U, int
     }
 }
 
+// The whole unit in one thread: 2-D table, bra and ket transfers, with plain
+// incrementing loops (the level-parallel phases above decode every element's
+// indices, which costs more than the arithmetic for small units).
+template <class C>
+QX_HD inline void rys_phase_units(const RysPrim& s, const double* uw, int rb0, int nrb, double* U, int tid, int nth) {
+    for (int u = tid; u < 3 * nrb; u += nth) {
+        const int x = u % 3, r = rb0 + u / 3;
+        const double t2 = uw[r];
+        const double B00 = 0.5 * t2 * s.rs;
+        const double B10 = 0.5 / s.p * (1.0 - t2 * s.q * s.rs);
+        const double B01 = 0.5 / s.q * (1.0 - t2 * s.p * s.rs);
+        const double C00 = s.PA[x] - t2 * s.q * s.rs * s.PQ[x];
+        const double D00 = s.QC[x] + t2 * s.p * s.rs * s.PQ[x];
+        const double AB = s.AB[x], CD = s.CD[x];
+        double* g = U + (size_t)u * C::USZ;  // level b: g[(b * NI + a) * NK + k]
+        g[0] = x == 2 ? uw[C::NR + r] : 1.0;
+        if (C::NI > 1) g[C::NK] = C00 * g[0];
+        for (int i = 2; i < C::NI; ++i) g[i * C::NK] = C00 * g[(i - 1) * C::NK] + (i - 1) * B10 * g[(i - 2) * C::NK];
+        for (int k = 1; k < C::NK; ++k) {
+            const double kB01 = (k - 1) * B01;
+            g[k] = D00 * g[k - 1] + (k > 1 ? kB01 * g[k - 2] : 0.0);
+            for (int i = 1; i < C::NI; ++i)
+                g[i * C::NK + k] = D00 * g[i * C::NK + k - 1] + (k > 1 ? kB01 * g[i * C::NK + k - 2] : 0.0) +
+                                   i * B00 * g[(i - 1) * C::NK + k - 1];
+        }
+        for (int b = 1; b < C::B1; ++b) {
+            const double* gp = g + (b - 1) * C::NI * C::NK;
+            double* gc = g + b * C::NI * C::NK;
+            for (int a = 0; a < C::NI - b; ++a)
+                for (int k = 0; k < C::NK; ++k) gc[a * C::NK + k] = gp[(a + 1) * C::NK + k] + AB * gp[a * C::NK + k];
+        }
+        double* h = g + C::SBRA;  // [a][b][d][c]
+        for (int a = 0; a < C::A1; ++a)
+            for (int b = 0; b < C::B1; ++b) {
+                double* hb = h + (a * C::B1 + b) * C::D1 * C::NK;
+                const double* src = g + (b * C::NI + a) * C::NK;
+                for (int c = 0; c < C::NK; ++c) hb[c] = src[c];
+                for (int d = 1; d < C::D1; ++d)
+                    for (int c = 0; c < C::NK - d; ++c)
+                        hb[d * C::NK + c] = hb[(d - 1) * C::NK + c + 1] + CD * hb[(d - 1) * C::NK + c];
+            }
+    }
+}
+
 // One op (per-centre derivative orders k[4]) of a unit at the unraised point
 // (a, b, c, d) from the raised table.
 template <class C>
@@ -507,6 +557,35 @@ QX_HD inline int rys_comp_offsets(int kc) {
     return packed;
 }
 
+// Cartesian exponents (a, b, c) of component kc in the three directions, packed
+// 2 bits each, 6 bits per direction (the factors of d g_i = 2e g_{i+1} - i g_{i-1}).
+template <class C, int LA, int LB, int LC, int LD>
+QX_HD inline int rys_comp_exps(int kc) {
+    constexpr int NB = C::NB, NC = C::NC, ND = C::ND;
+    const int ic = (kc / ND) % NC, ib = (kc / (ND * NC)) % NB, ia = kc / (ND * NC * NB);
+    int ea[3], eb[3], ec[3];
+    cart_exps(LA, ia, ea[0], ea[1], ea[2]);
+    cart_exps(LB, ib, eb[0], eb[1], eb[2]);
+    cart_exps(LC, ic, ec[0], ec[1], ec[2]);
+    int p = 0;
+    for (int x = 0; x < 3; ++x) p |= (ea[x] | eb[x] << 2 | ec[x] << 4) << (6 * x);
+    return p;
+}
+
+// First derivatives of one direction's factor from the raw table at offset o
+// (exponents e = a | b << 2 | c << 4): dA, dB, dC.
+template <class C>
+QX_HD inline void rys_raw_d1(const double* T, int o, int e, const double* e2, double& dA, double& dB, double& dC) {
+    constexpr int SA = C::B1 * C::D1 * C::NK, SB = C::D1 * C::NK;
+    const int a = e & 3, b = (e >> 2) & 3, c = (e >> 4) & 3;
+    dA = e2[0] * T[o + SA];
+    if (a) dA -= a * T[o - SA];
+    dB = e2[1] * T[o + SB];
+    if (b) dB -= b * T[o - SB];
+    dC = e2[2] * T[o + 1];
+    if (c) dC -= c * T[o - 1];
+}
+
 // Plain kind: add the batch's products of component kc (packed offsets).
 template <class C>
 QX_HD inline double rys_prod_plain(const double* U, int nrb, int off) {
@@ -519,23 +598,22 @@ QX_HD inline double rys_prod_plain(const double* U, int nrb, int off) {
     return s;
 }
 
-// Gradient kind: g[3X + i] += gam * sum_r (dX I)_i prod_{j != i} I_j, X = A, B, C.
+// Gradient kind: g[3X + i] += gam * sum_r (dX I)_i prod_{j != i} I_j, X = A, B, C,
+// the derivatives formed from the raw tables of the batch's units.
 template <class C>
-QX_HD inline void rys_prod_grad(const double* O, int nrb, int off, double gam, double* g) {
-    const int ox = off & 1023, oy = (off >> 10) & 1023, oz = off >> 20;
-    constexpr int S = C::SZ0;
+QX_HD inline void rys_prod_grad(const double* U, int nrb, int off, int ex, const double* e2, double gam, double* g) {
+    const int o[3] = {off & 1023, (off >> 10) & 1023, off >> 20};
     for (int r = 0; r < nrb; ++r) {
-        const double* X = O + (size_t)3 * r * C::UOPS;
-        const double* Y = X + C::UOPS;
-        const double* Z = Y + C::UOPS;
-        const double Ix = X[ox], Iy = Y[oy], Iz = Z[oz];
-        const double gz = gam * Iz;
-        const double yz = Iy * gz, xz = Ix * gz, xy = Ix * Iy * gam;
+        const double* T = U + (size_t)3 * r * C::USZ + C::SBRA;
+        const double I[3] = {T[o[0]], T[C::USZ + o[1]], T[2 * C::USZ + o[2]]};
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            g[3 * c + 0] = fma(X[(c + 1) * S + ox], yz, g[3 * c + 0]);
-            g[3 * c + 1] = fma(Y[(c + 1) * S + oy], xz, g[3 * c + 1]);
-            g[3 * c + 2] = fma(Z[(c + 1) * S + oz], xy, g[3 * c + 2]);
+        for (int x = 0; x < 3; ++x) {
+            double dA, dB, dC;
+            rys_raw_d1<C>(T + x * C::USZ, o[x], (ex >> (6 * x)) & 63, e2, dA, dB, dC);
+            const double w = gam * (x == 0 ? I[1] * I[2] : (x == 1 ? I[0] * I[2] : I[0] * I[1]));
+            g[x] = fma(dA, w, g[x]);
+            g[3 + x] = fma(dB, w, g[3 + x]);
+            g[6 + x] = fma(dC, w, g[6 + x]);
         }
     }
 }
@@ -543,22 +621,24 @@ QX_HD inline void rys_prod_grad(const double* O, int nrb, int off, double gam, d
 // Gradient-tile kind: acc[b - b0] += sum_r (dX I)_i prod_{j != i} I_j for the
 // derivative coordinates b = 3X + i in [b0, b0 + GG).
 template <class C>
-QX_HD inline void rys_prod_gradt(const double* O, int nrb, int off, int b0, double* acc) {
+QX_HD inline void rys_prod_gradt(const double* U, int nrb, int off, int ex, const double* e2, int b0, double* acc) {
     const int o[3] = {off & 1023, (off >> 10) & 1023, off >> 20};
-    constexpr int S = C::SZ0;
     for (int r = 0; r < nrb; ++r) {
         const double* T[3];
-        T[0] = O + (size_t)3 * r * C::UOPS;
-        T[1] = T[0] + C::UOPS;
-        T[2] = T[1] + C::UOPS;
+        T[0] = U + (size_t)3 * r * C::USZ + C::SBRA;
+        T[1] = T[0] + C::USZ;
+        T[2] = T[1] + C::USZ;
         const double I[3] = {T[0][o[0]], T[1][o[1]], T[2][o[2]]};
+        double dd[3][3];
+#pragma unroll
+        for (int x = 0; x < 3; ++x) rys_raw_d1<C>(T[x], o[x], (ex >> (6 * x)) & 63, e2, dd[x][0], dd[x][1], dd[x][2]);
 #pragma unroll
         for (int g = 0; g < C::GG; ++g) {
             const int b = b0 + g;
             if (b >= 9) break;
             const int X = b / 3, i = b - 3 * X;
             const double other = i == 0 ? I[1] * I[2] : (i == 1 ? I[0] * I[2] : I[0] * I[1]);
-            acc[g] = fma(T[i][(X + 1) * S + o[i]], other, acc[g]);
+            acc[g] = fma(dd[i][X], other, acc[g]);
         }
     }
 }
@@ -717,7 +797,7 @@ __device__ __forceinline__ double rys_team_max(double v, double* red, int tid, i
 }
 
 // Per primitive quartet: nodes/weights, then per root batch the tables and the
-// caller's product step `prod(U, O, nrb)`.
+// caller's product step `prod(nrb, e2)` (e2: twice the four exponents).
 template <class C, int KIND, int LA, int LB, int LC, int LD, class Prod>
 __device__ __forceinline__ void rys_primitive(const RysArgs& ra, const PrimPair& p, const PrimPair& r,
                                               const PairInfo& P, const PairInfo& Q, double* uw, double* U, double* O,
@@ -729,21 +809,26 @@ __device__ __forceinline__ void rys_primitive(const RysArgs& ra, const PrimPair&
     for (int rb0 = 0; rb0 < C::NR; rb0 += C::RB) {
         const int nrb = C::NR - rb0 < C::RB ? C::NR - rb0 : C::RB;
         if (rb0) rys_team_sync<C::TS, C::TPB>(team);  // the previous batch's products are done
-        rys_phase_2d<C>(s, uw, rb0, nrb, U, tid, C::TS);
-        rys_team_sync<C::TS, C::TPB>(team);
-        for (int b = 1; b < C::B1; ++b) {
-            rys_phase_bra<C>(s, b, nrb, U, tid, C::TS);
+        if constexpr (C::SEQ) {
+            rys_phase_units<C>(s, uw, rb0, nrb, U, tid, C::TS);
             rys_team_sync<C::TS, C::TPB>(team);
-        }
-        for (int d = 0; d < C::D1; ++d) {
-            rys_phase_ket<C>(s, d, nrb, U, tid, C::TS);
+        } else {
+            rys_phase_2d<C>(s, uw, rb0, nrb, U, tid, C::TS);
             rys_team_sync<C::TS, C::TPB>(team);
+            for (int b = 1; b < C::B1; ++b) {
+                rys_phase_bra<C>(s, b, nrb, U, tid, C::TS);
+                rys_team_sync<C::TS, C::TPB>(team);
+            }
+            for (int d = 0; d < C::D1; ++d) {
+                rys_phase_ket<C>(s, d, nrb, U, tid, C::TS);
+                rys_team_sync<C::TS, C::TPB>(team);
+            }
         }
         if constexpr (C::NOPS > 0) {
             rys_phase_ops<C, KIND, LA, LB, LC, LD>(s, nrb, U, O, w9, tid, C::TS);
             rys_team_sync<C::TS, C::TPB>(team);
         }
-        prod(nrb);
+        prod(nrb, s.e2);
     }
     rys_team_sync<C::TS, C::TPB>(team);  // products done before the next nodes overwrite
 }
@@ -812,11 +897,14 @@ __global__ void __launch_bounds__(RysCls<LA, LB, LC, LD, KIND>::BS)
         }
         // components of this thread
         int offs[NCPT];
+        int exps[NCPT];
         double gam[NCPT];
 #pragma unroll
         for (int j = 0; j < NCPT; ++j) {
             const int kc = tid + j * TS;
-            offs[j] = kc < C::NCOMP ? rys_comp_offsets<C, LA, LB, LC, LD, KIND == RK_PLAIN>(kc) : 0;
+            offs[j] = kc < C::NCOMP ? rys_comp_offsets<C, LA, LB, LC, LD, C::RAW>(kc) : 0;
+            if constexpr (KIND == RK_GRAD || KIND == RK_GRADT)
+                exps[j] = kc < C::NCOMP ? rys_comp_exps<C, LA, LB, LC, LD>(kc) : 0;
             gam[j] = 0.0;
             if constexpr (KIND == RK_GRAD || KIND == RK_HVP) {
                 if (kc < C::NCOMP) {
@@ -846,7 +934,7 @@ __global__ void __launch_bounds__(RysCls<LA, LB, LC, LD, KIND>::BS)
             for (int t = 0; t < ntot; ++t) {
                 const int i = t / nk, jj = t - i * nk;
                 rys_primitive<C, KIND, LA, LB, LC, LD>(ra, a.prims[P.prim_off + i], a.prims[Q.prim_off + jj], P, Q,
-                                                        uw, U, O, w9, tid, team, [&](int nrb) {
+                                                        uw, U, O, w9, tid, team, [&](int nrb, const double*) {
 #pragma unroll
                     for (int j = 0; j < NCPT; ++j)
                         if (tid + j * TS < C::NCOMP) acc[j] += rys_prod_plain<C>(U, nrb, offs[j]);
@@ -893,10 +981,11 @@ __global__ void __launch_bounds__(RysCls<LA, LB, LC, LD, KIND>::BS)
                 for (int t = 0; t < ntot; ++t) {
                     const int i = t / nk, jj = t - i * nk;
                     rys_primitive<C, KIND, LA, LB, LC, LD>(ra, a.prims[P.prim_off + i], a.prims[Q.prim_off + jj], P,
-                                                            Q, uw, U, O, w9, tid, team, [&](int nrb) {
+                                                            Q, uw, U, O, w9, tid, team, [&](int nrb, const double* e2) {
 #pragma unroll
                         for (int j = 0; j < NCPT; ++j)
-                            if (tid + j * TS < C::NCOMP) rys_prod_gradt<C>(O, nrb, offs[j], b0, acc[j]);
+                            if (tid + j * TS < C::NCOMP)
+                                rys_prod_gradt<C>(U, nrb, offs[j], exps[j], e2, b0, acc[j]);
                     });
                 }
 #pragma unroll
@@ -921,12 +1010,12 @@ __global__ void __launch_bounds__(RysCls<LA, LB, LC, LD, KIND>::BS)
             for (int t = 0; t < ntot; ++t) {
                 const int i = t / nk, jj = t - i * nk;
                 rys_primitive<C, KIND, LA, LB, LC, LD>(ra, a.prims[P.prim_off + i], a.prims[Q.prim_off + jj], P, Q,
-                                                        uw, U, O, w9, tid, team, [&](int nrb) {
+                                                        uw, U, O, w9, tid, team, [&](int nrb, const double* e2) {
 #pragma unroll
                     for (int j = 0; j < NCPT; ++j)
                         if (tid + j * TS < C::NCOMP) {
                             if constexpr (KIND == RK_GRAD)
-                                rys_prod_grad<C>(O, nrb, offs[j], gam[j], g);
+                                rys_prod_grad<C>(U, nrb, offs[j], exps[j], e2, gam[j], g);
                             else
                                 rys_prod_hvp<C>(O, nrb, offs[j], gam[j], g);
                         }
@@ -956,7 +1045,7 @@ __global__ void __launch_bounds__(RysCls<LA, LB, LC, LD, KIND>::BS)
                 for (int t = 0; t < ntot; ++t) {
                     const int i = t / nk, jj = t - i * nk;
                     rys_primitive<C, KIND, LA, LB, LC, LD>(ra, a.prims[P.prim_off + i], a.prims[Q.prim_off + jj], P,
-                                                            Q, uw, U, O, w9, tid, team, [&](int nrb) {
+                                                            Q, uw, U, O, w9, tid, team, [&](int nrb, const double*) {
 #pragma unroll
                         for (int j = 0; j < NCPT; ++j)
                             if (tid + j * TS < C::NCOMP)
