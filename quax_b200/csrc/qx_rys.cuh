@@ -124,6 +124,13 @@ struct RysCls {
     static constexpr int TEAM_SMEM = HDR + RB * PER_ROOT;  // doubles
     static constexpr int SMEM = TPB * TEAM_SMEM * 8;       // bytes per block
     static constexpr bool FITS = SMEM <= RYS_SMEM_MAX;
+    // minimum blocks per SM for the register budget: one for the 256-thread
+    // classes, which need the full 255 registers (left to its own heuristics the
+    // compiler gives some of them 64-80 registers and kilobytes of spills, and
+    // those builds returned wrong gradients for (33|32)); the compiler's choice
+    // (0) for 128-thread blocks, measured faster than capping them at 170
+    // registers for three blocks per SM
+    static constexpr int MINB = BS >= 256 ? 1 : 0;
     // offsets of one component in a table are packed 10 bits per direction
     // products read the raw transferred table (plain and gradient kinds) or the
     // op tables (the others)
@@ -834,7 +841,7 @@ __device__ __forceinline__ void rys_primitive(const RysArgs& ra, const PrimPair&
 }
 
 template <int LA, int LB, int LC, int LD, int KIND>
-__global__ void __launch_bounds__(RysCls<LA, LB, LC, LD, KIND>::BS)
+__global__ void __launch_bounds__(RysCls<LA, LB, LC, LD, KIND>::BS, RysCls<LA, LB, LC, LD, KIND>::MINB)
     k_rys(RysArgs ra, int mode, long long nwork) {
     using C = RysCls<LA, LB, LC, LD, KIND>;
     constexpr int TS = C::TS, TPB = C::TPB, NCPT = C::NCPT;
