@@ -1111,7 +1111,8 @@ class _Out:
 
 # Highest shell angular momentum of the Rys engine (every class up to (ff|ff)).
 RYS_LMAX = 3
-RYS_ALL_KINDS = ("RK_PLAIN", "RK_GRAD", "RK_HVP", "RK_GRADT", "RK_DER1", "RK_DER2", "RK_DER3", "RK_DER4")
+RYS_ALL_KINDS = ("RK_PLAIN", "RK_GRAD", "RK_GRADL", "RK_HVP", "RK_GRADT", "RK_DER1", "RK_DER2", "RK_DER3",
+                 "RK_DER4")
 
 
 def gen_rys(here, lmax_os):

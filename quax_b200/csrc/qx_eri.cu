@@ -263,6 +263,7 @@ struct qx_handle {
     int deriv_eng[QX_NCLS_ALL];
     int wpq[QX_NCLS_ALL];        // warps per quartet, plain warp kernels
     int wpq_deriv[QX_NCLS_ALL];  // warps per quartet, derivative warp kernels
+    int rys_lp[QX_NCLS_ALL];     // Rys adjoint gradient: 1 = level-parallel table build (RK_GRADL)
     int shard_rank = 0, shard_n = 1;
     int prim_stage = 0;  // split-mode VRR: primitive pairs staged per warp (2 x largest pair), 0 = off
     int wait_limit = 1 << 22;  // polls of the bounded waits on those staging copies
@@ -537,7 +538,10 @@ extern "C" int qx_initialize(int natom, const double* coords, int nshell, const 
     qx_handle* h = new qx_handle();
     cudaGetDevice(&h->device);
     choose_engines(h);
-    for (int c = 0; c < QX_NCLS_ALL; ++c) h->wpq[c] = h->wpq_deriv[c] = 1;
+    for (int c = 0; c < QX_NCLS_ALL; ++c) {
+        h->wpq[c] = h->wpq_deriv[c] = 1;
+        h->rys_lp[c] = 0;
+    }
     h->natom = natom;
     h->nshell = nshell;
     h->pure = pure;
@@ -1094,7 +1098,8 @@ static int run_rys_contract(qx_handle* h, int c, int kind, const double* D, doub
     ra.grad = grad;
     ra.dir = dir;
     ra.M = 3 * h->natom;
-    if (g_rys_launch[c](ra, kind, 0, w.nq, cs)) return rys_unsupported(c, kind == RK_GRAD ? "gradient" : "Hessian");
+    if (kind == RK_GRAD && h->rys_lp[c]) kind = RK_GRADL;
+    if (g_rys_launch[c](ra, kind, 0, w.nq, cs)) return rys_unsupported(c, kind == RK_HVP ? "Hessian" : "gradient");
     QX_CUDA(cudaGetLastError());
     return QX_OK;
 }
@@ -1534,8 +1539,8 @@ extern "C" int qx_autotune(qx_handle* h, int what, void* stream) {
         rc = fail(QX_E_CUDA, "qx_autotune: memset failed");
     for (int c = 0; c < QX_NCLS_ALL && !rc; ++c) {
         ClassWork& w = h->work[c];
-        if (!w.nq || !has_os(c)) continue;  // the Rys classes have one engine
-        if (what & 1) {
+        if (!w.nq) continue;
+        if ((what & 1) && has_os(c)) {  // the f classes have one plain engine
             std::vector<TuneCfg> cand;
             if (!g_class_coop[c] && !g_class_scratch[c])
                 for (int lg = 0; lg <= 5; ++lg) cand.push_back({ENG_SL, lg});
@@ -1577,12 +1582,14 @@ extern "C" int qx_autotune(qx_handle* h, int what, void* stream) {
             if (g_has_wvrr[c]) cand.push_back({ENG_WVRR, 0});
             if (g_has_dsplit[c]) cand.push_back({ENG_DSPLIT, 0});
             if (g_der_idx[c] >= 0) cand.push_back({ENG_COOP, 0});
-            cand.push_back({ENG_RYS, 0});
+            cand.push_back({ENG_RYS, 0});  // Rys, per-unit table build for small units
+            cand.push_back({ENG_RYS, 1});  // Rys, level-parallel table build
             float best = 1e30f;
-            TuneCfg bc{h->deriv_eng[c], h->wpq_deriv[c]};
+            TuneCfg bc{h->deriv_eng[c], h->deriv_eng[c] == ENG_RYS ? h->rys_lp[c] : h->wpq_deriv[c]};
             for (const TuneCfg& t : cand) {
                 h->deriv_eng[c] = t.eng;
                 if (t.eng == ENG_WARP) h->wpq_deriv[c] = t.param;
+                if (t.eng == ENG_RYS) h->rys_lp[c] = t.param;
                 float ms = 0.f;
                 rc = time_config(s, e0, e1, &ms, [&] {
                     return run_deriv_class(h, c, QX_MODE_GRAD, nullptr, d_D, 1.0, -0.5, d_g, -1, s);
@@ -1595,6 +1602,7 @@ extern "C" int qx_autotune(qx_handle* h, int what, void* stream) {
             }
             h->deriv_eng[c] = bc.eng;
             if (bc.eng == ENG_WARP) h->wpq_deriv[c] = bc.param;
+            h->rys_lp[c] = bc.eng == ENG_RYS ? bc.param : 0;
         }
     }
     if (!rc) {
@@ -1613,7 +1621,9 @@ extern "C" int qx_autotune(qx_handle* h, int what, void* stream) {
 // Engine of one class chosen by the caller (tests, measurements): the autotuner's
 // choice made by hand.  plain / deriv: engine ids as qx_engine_config reports
 // them, -1 keeps the current one; pparam / dparam: log2 lanes per quartet
-// (straight-line) or warps per quartet (warp kernels), ignored otherwise.
+// (straight-line) or warps per quartet (warp kernels); for the Rys derivative
+// engine dparam 0 or 1 picks the adjoint gradient's table build (per-unit for
+// small units, or level-parallel); ignored otherwise.
 extern "C" int qx_set_engine(qx_handle* h, int cls, int plain, int pparam, int deriv, int dparam) {
     if (!h || cls < 0 || cls >= QX_NCLS_ALL) return fail(QX_E_INVALID, "qx_set_engine: bad handle or class");
     DeviceGuard g(h->device);
@@ -1657,10 +1667,11 @@ extern "C" int qx_set_engine(qx_handle* h, int cls, int plain, int pparam, int d
         if (deriv == ENG_WVRR) ok = has_os(cls) && g_has_wvrr[cls];
         if (deriv == ENG_DSPLIT) ok = has_os(cls) && g_has_dsplit[cls];
         if (deriv == ENG_COOP) ok = g_der_idx[cls] >= 0;
-        if (deriv == ENG_RYS) ok = true;
+        if (deriv == ENG_RYS) ok = dparam == 0 || dparam == 1;
         if (!ok) return no("derivative", deriv);
         h->deriv_eng[cls] = deriv;
         if (deriv == ENG_WARP) h->wpq_deriv[cls] = dparam;
+        if (deriv == ENG_RYS) h->rys_lp[cls] = dparam;
     }
     return QX_OK;
 }
@@ -1699,7 +1710,7 @@ extern "C" int qx_engine_config(const qx_handle* h, int cls, int* cfg) {
     cfg[0] = h->plain_eng[cls];
     cfg[1] = h->plain_eng[cls] == ENG_SL ? h->work[cls].log2g : (h->plain_eng[cls] == ENG_WARP ? h->wpq[cls] : 0);
     cfg[2] = h->deriv_eng[cls];
-    cfg[3] = h->deriv_eng[cls] == ENG_WARP ? h->wpq_deriv[cls] : 0;
+    cfg[3] = h->deriv_eng[cls] == ENG_WARP ? h->wpq_deriv[cls] : (h->deriv_eng[cls] == ENG_RYS ? h->rys_lp[cls] : 0);
     return QX_OK;
 }
 

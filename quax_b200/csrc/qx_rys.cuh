@@ -25,10 +25,13 @@
 // barriers) owns one contracted quartet at a time and walks its primitive
 // quartets.  Per primitive quartet: 2n threads evaluate the nodes/weights, then
 // per batch of RB roots the 3*RB (direction, root) units build their 2-D tables
-// (one thread per unit), the transfer levels run in parallel over the team, the
-// derivative tables are formed (derivative kinds), and every thread adds the
-// products for its own Cartesian components into registers.  All tables live in
-// shared memory; nothing is written to global memory until the epilogue.
+// (one thread per unit) and the transfer levels run -- in parallel over the team
+// level by level, or, for small units, the whole unit in the thread that built
+// its 2-D table -- the derivative tables are formed (higher-order kinds; the
+// first-derivative kinds form dA, dB, dC from the raw table inside the
+// products), and every thread adds the products for its own Cartesian
+// components into registers.  All tables live in shared memory; nothing is
+// written to global memory until the epilogue.
 #pragma once
 #include "qx_warp.cuh"
 #include "qx_rys_table.inc"
@@ -48,8 +51,11 @@ constexpr int RYS_TABLE_DOUBLES = QX_RYS_TAB_SIZE + 2 * QX_RYS_ASYM_SIZE;
 // Kinds of Rys programs: which centres are raised for derivatives, the
 // derivative order the quadrature must integrate, and the per-direction 1-D
 // derivative tables the products read.
-enum { RK_PLAIN = 0, RK_GRAD = 1, RK_HVP = 2, RK_GRADT = 3, RK_DER1 = 11, RK_DER2 = 12, RK_DER3 = 13,
-       RK_DER4 = 14 };
+enum { RK_PLAIN = 0, RK_GRAD = 1, RK_HVP = 2, RK_GRADT = 3, RK_GRADL = 4, RK_DER1 = 11, RK_DER2 = 12,
+       RK_DER3 = 13, RK_DER4 = 14 };
+// The adjoint-gradient kinds: RK_GRADL is RK_GRAD with every unit's tables built
+// level by level over the team (the autotuner picks the faster build per class).
+QX_HD constexpr bool rys_is_grad(int kind) { return kind == RK_GRAD || kind == RK_GRADL; }
 // Epilogues of the plain kind (the derivative kinds have their own).
 enum { RMODE_DENSE = 0, RMODE_UNIQUE = 1, RMODE_SCHWARZ = 2, RMODE_JK = 3 };
 
@@ -74,6 +80,8 @@ template <>
 struct RysKind<RK_GRAD> {  // A, B, C raised by one; dA, dB, dC formed in the products (D by invariance)
     static constexpr int ORD = 1, KA = 1, KB = 1, KC = 1, KD = 0, NOPS = 0;
 };
+template <>
+struct RysKind<RK_GRADL> : RysKind<RK_GRAD> {};
 template <>
 struct RysKind<RK_GRADT> {  // as RK_GRAD, but the 9 derivative integrals are written to a tile
     static constexpr int ORD = 1, KA = 1, KB = 1, KC = 1, KD = 0, NOPS = 0;
@@ -134,11 +142,11 @@ struct RysCls {
     // offsets of one component in a table are packed 10 bits per direction
     // products read the raw transferred table (plain and gradient kinds) or the
     // op tables (the others)
-    static constexpr bool RAW = KIND == RK_PLAIN || KIND == RK_GRAD || KIND == RK_GRADT;
+    static constexpr bool RAW = KIND == RK_PLAIN || rys_is_grad(KIND) || KIND == RK_GRADT;
     static_assert((!RAW || SRAW < 1024) && SZ0 < 1024, "1-D table offsets exceed 10 bits");
     // one thread builds a whole (direction, root) unit -- 2-D table and both
     // transfers -- when the units keep at least a sixth of the team busy or are small
-    static constexpr bool SEQ = 6 * RB >= TS || SRAW <= 160;
+    static constexpr bool SEQ = KIND != RK_GRADL && (6 * RB >= TS || SRAW <= 160);
     // derivative tensors: multi-indices accumulated per pass over the primitives
     static constexpr int MG = NCPT >= 32 ? 1 : (32 / NCPT > 8 ? 8 : 32 / NCPT);
     // gradient tile: derivative coordinates (of the 9) accumulated per pass
@@ -431,10 +439,10 @@ QX_HD inline double rys_op_value(const RysPrim& s, double* U, int u, const int* 
 }
 
 // Op tables of the derivative kinds: O holds per unit NOPS tables of SZ0
-// entries [a][b][c][d] (unraised extents).  kind RK_GRAD: I, dA, dB, dC;
-// RK_DERk: every (ka, kb, kc, kd) with sum <= k in rys_op_rank order; RK_HVP:
-// I, dA, dB, dC, V, dA V, dB V, dC V with V = sum_X w_X dX along the
-// direction w (per unit direction: w9[3 * X + direction]).
+// entries [a][b][c][d] (unraised extents).  RK_DERk: every (ka, kb, kc, kd)
+// with sum <= k in rys_op_rank order; RK_HVP: I, dA, dB, dC, V, dA V, dB V, dC V
+// with V = sum_X w_X dX along the direction w (per unit direction:
+// w9[3 * X + direction]).
 template <class C, int KIND, int LA, int LB, int LC, int LD>
 QX_HD inline void rys_phase_ops(const RysPrim& s, int nrb, double* U, double* O, const double* w9, int tid, int nth) {
     constexpr int per = C::NOPS * C::SZ0;
@@ -444,19 +452,7 @@ QX_HD inline void rys_phase_ops(const RysPrim& s, int nrb, double* U, double* O,
         const int d = el % (LD + 1), c = (el / (LD + 1)) % (LC + 1), b = (el / ((LD + 1) * (LC + 1))) % (LB + 1),
                   a = el / ((LD + 1) * (LC + 1) * (LB + 1));
         double v;
-        if constexpr (KIND == RK_GRAD || KIND == RK_GRADT) {
-            // closed forms: I, and dX g = 2 e_X g(x+1) - x g(x-1) for X = A, B, C
-            auto R = [&](int ia, int ib, int ic) { return rys_gk<C>(U, u, ia, ib, d, ic); };
-            if (op == 0) {
-                v = R(a, b, c);
-            } else if (op == 1) {
-                v = s.e2[0] * R(a + 1, b, c) - (a ? a * R(a - 1, b, c) : 0.0);
-            } else if (op == 2) {
-                v = s.e2[1] * R(a, b + 1, c) - (b ? b * R(a, b - 1, c) : 0.0);
-            } else {
-                v = s.e2[2] * R(a, b, c + 1) - (c ? c * R(a, b, c - 1) : 0.0);
-            }
-        } else if constexpr (KIND == RK_HVP) {
+        if constexpr (KIND == RK_HVP) {
             // first and second derivatives on A, B, C in closed form: per centre the
             // index shifts by +-1 (+-2 for a repeated centre) with the factors of
             // d g_i = e2 g_{i+1} - i g_{i-1}
@@ -910,10 +906,10 @@ __global__ void __launch_bounds__(RysCls<LA, LB, LC, LD, KIND>::BS, RysCls<LA, L
         for (int j = 0; j < NCPT; ++j) {
             const int kc = tid + j * TS;
             offs[j] = kc < C::NCOMP ? rys_comp_offsets<C, LA, LB, LC, LD, C::RAW>(kc) : 0;
-            if constexpr (KIND == RK_GRAD || KIND == RK_GRADT)
+            if constexpr (rys_is_grad(KIND) || KIND == RK_GRADT)
                 exps[j] = kc < C::NCOMP ? rys_comp_exps<C, LA, LB, LC, LD>(kc) : 0;
             gam[j] = 0.0;
-            if constexpr (KIND == RK_GRAD || KIND == RK_HVP) {
+            if constexpr (rys_is_grad(KIND) || KIND == RK_HVP) {
                 if (kc < C::NCOMP) {
                     const int id = kc % C::ND, ic = (kc / C::ND) % C::NC, ib = (kc / (C::ND * C::NC)) % C::NB,
                               ia = kc / (C::ND * C::NC * C::NB);
@@ -1010,7 +1006,7 @@ __global__ void __launch_bounds__(RysCls<LA, LB, LC, LD, KIND>::BS, RysCls<LA, L
                     }
                 }
             }
-        } else if constexpr (KIND == RK_GRAD || KIND == RK_HVP) {
+        } else if constexpr (rys_is_grad(KIND) || KIND == RK_HVP) {
             double g[9];
 #pragma unroll
             for (int b = 0; b < 9; ++b) g[b] = 0.0;
@@ -1021,7 +1017,7 @@ __global__ void __launch_bounds__(RysCls<LA, LB, LC, LD, KIND>::BS, RysCls<LA, L
 #pragma unroll
                     for (int j = 0; j < NCPT; ++j)
                         if (tid + j * TS < C::NCOMP) {
-                            if constexpr (KIND == RK_GRAD)
+                            if constexpr (rys_is_grad(KIND))
                                 rys_prod_grad<C>(U, nrb, offs[j], exps[j], e2, gam[j], g);
                             else
                                 rys_prod_hvp<C>(O, nrb, offs[j], gam[j], g);

@@ -212,7 +212,9 @@ class EriEngine:
                    deriv_param: int = 0) -> None:
         """Force the engine of one class (names as in ENGINE_NAMES; None keeps the
         current one).  plain_param: log2 lanes per quartet ("sl") or warps per
-        quartet ("warp": 1 or 4); deriv_param: warps per quartet ("warp")."""
+        quartet ("warp": 1 or 4); deriv_param: warps per quartet ("warp"), or the
+        Rys adjoint gradient's table build ("rys": 0 per-unit for small units, 1
+        level-parallel)."""
         pe = -1 if plain is None else self.ENGINE_NAMES.index(plain)
         de = -1 if deriv is None else self.ENGINE_NAMES.index(deriv)
         with torch.cuda.device(self.device):

@@ -25,7 +25,7 @@ import torch
 pytestmark = pytest.mark.gpu
 
 PLAIN = [("sl", lg) for lg in range(6)] + [("warp", 1), ("warp", 4), ("coop", 0), ("wsplit", 1), ("rys", 0)]
-DERIV = [("warp", 1), ("warp", 4), ("wvrr", 0), ("dsplit", 0), ("coop", 0), ("rys", 0)]
+DERIV = [("warp", 1), ("warp", 4), ("wvrr", 0), ("dsplit", 0), ("coop", 0), ("rys", 0), ("rys", 1)]
 
 
 @pytest.fixture(scope="module")

@@ -108,9 +108,16 @@ def test_f_deriv_core_and_slice(oracle_lib, seed):
 
 
 @pytest.mark.parametrize("seed", [0, 1])
-def test_f_grad_adjoint(oracle_lib, seed):
+@pytest.mark.parametrize("build", [None, 0, 1])
+def test_f_grad_adjoint(oracle_lib, seed, build):
+    """The adjoint gradient with the default engines, and with the Rys engine
+    forced on every class with either table build (per-unit for small units, or
+    level-parallel), against the oracle."""
     b = f_synthetic(seed)
     eng = _engine(b, 1e-12)
+    if build is not None:
+        for c in eng.class_info():
+            eng.set_engine(c["cls"], deriv="rys", deriv_param=build)
     D = density(eng.nbf, seed)
     g = eng.grad_adjoint(torch.from_numpy(D).cuda(), 1.0, -0.5).cpu().numpy()
     gr = oracle_lib.grad_contract(oracle_lib.OracleBasis(b), 1e-12, D, 1.0, -0.5)
