@@ -607,14 +607,20 @@ def batched_extras(count: int, iterations: int = 20):
 
 
 def run_grad_only(args):
-    """Adjoint gradient of the workload only (profiling aid; prints its timing)."""
+    """Adjoint gradient of the workload only (profiling aid; prints its timing).
+    With --profile-f: an 8-atom synthetic molecule with f shells on the heavy
+    atoms (the 60-atom workload's shell mix at a size a profiler replays quickly),
+    whose gradient is dominated by the Rys kernels of the f classes."""
     import numpy as np
     import torch
 
-    from quax_b200.basis import config_spec, synthetic_molecule
+    from quax_b200.basis import SyntheticSpec, config_spec, synthetic_molecule
     from quax_b200.integrals.engine import EriEngine
 
-    mol, b = synthetic_molecule(config_spec(WORKLOAD), 0)
+    if args.profile_f:
+        mol, b = synthetic_molecule(SyntheticSpec(natom=8, f_shell=True), 0)
+    else:
+        mol, b = synthetic_molecule(config_spec(WORKLOAD), 0)
     eng = EriEngine(b, THR)
     eng.autotune(plain=False, deriv=True)
     n = eng.nbf
@@ -632,8 +638,23 @@ def run_grad_only(args):
     e1.record()
     torch.cuda.synchronize()
     torch.cuda.profiler.stop()
-    print(json.dumps({"adjoint_ms": e0.elapsed_time(e1) / args.steps, "note": "--profile-grad",
-                      "engine_config": eng.engine_config()}), flush=True)
+    ms = e0.elapsed_time(e1) / args.steps
+    # per class (outside the profiled region): one event-timed evaluation and the
+    # algorithmic first-derivative FLOPs qx_class_info reports
+    g = torch.zeros(3 * eng.natom, dtype=torch.float64, device="cuda")
+    classes = {}
+    for c in eng.class_info():
+        if not c["nq"]:
+            continue
+        e0.record()
+        eng.grad_adjoint_class(c["cls"], D, g)
+        e1.record()
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1)
+        classes["%d%d%d%d" % c["l"]] = {"ms": t, "gflop": c["flops_deriv"] * 1e-9,
+                                        "tflops": c["flops_deriv"] / (t * 1e-3) * 1e-12}
+    print(json.dumps({"adjoint_ms": ms, "note": "--profile-grad", "engine_config": eng.engine_config(),
+                      "classes": classes}), flush=True)
 
 
 # ------------------------------------------------------------- reference arm ---
@@ -687,6 +708,8 @@ def main():
                     help="displaced geometries in the batched-RHF extra (the full workload is 256)")
     ap.add_argument("--profile-grad", action="store_true",
                     help="run only the adjoint gradient of the workload, warmup+steps times (for profiler runs)")
+    ap.add_argument("--profile-f", action="store_true",
+                    help="with --profile-grad: an 8-atom molecule with f shells instead of the workload")
     ap.add_argument("--no-extras", action="store_true",
                     help="time the ERI steps only (for profiler runs): no roofline probe, e2e, gradient or CPU arm")
     args = ap.parse_args()
