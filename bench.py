@@ -321,7 +321,7 @@ def run_ours(args):
     del host
 
     # the same molecule with spherical d shells (the synthetic workload's basis):
-    # Cartesian kernels + per-class solid-harmonic transforms (batched GEMMs)
+    # Cartesian kernels + the device solid-harmonic transform of every class
     from quax_b200.basis import Basis
     from quax_b200.integrals.spherical import SphericalEngine
 
@@ -337,7 +337,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     sph_ms = e0.elapsed_time(e1) / 3
     spherical = {"nbf": sph.nbf, "ms_per_step": sph_ms, "value": nq / (sph_ms * 1e-3), "unit": "quartets/s",
-                 "path": "Cartesian unique kernels + per-class solid-harmonic transforms (cuBLAS DGEMM)"}
+                 "path": "Cartesian unique kernels + per-class solid-harmonic transform kernel (qx_cart2sph_block)"}
     sph.close()
 
     grad = batched = None

@@ -264,6 +264,18 @@ int qx_deriv_tile(qx_handle *h, int cls, long long q0, long long q1, int images,
 int qx_gamma_tile(qx_handle *h, int cls, long long q0, long long q1, int images, const double *D, double cj,
                   double ck, double *gam, void *stream);
 
+/* Spherical blocks of one class of the unique layout.  No counterpart in the
+ * reference, whose Libint path is Cartesian (libint_interface.cc:47-73); it
+ * serves spherical bases on top of the Cartesian kernels.  in_dev holds the
+ * class's Cartesian unique blocks (ncart(la) ncart(lb) ncart(lc) ncart(ld) planes
+ * of nq doubles, as qx_eri_unique writes them), out_dev receives
+ * (2la+1)(2lb+1)(2lc+1)(2ld+1) planes of nq doubles in the same order.  T_host
+ * (host memory): the solid-harmonic matrices T_l, (2l+1) x ncart(l) row-major,
+ * for l = 0..QX_MAX_L, concatenated (110 doubles).  Allocates nothing;
+ * asynchronous on `stream`. */
+int qx_cart2sph_block(const double *in_dev, double *out_dev, const int *l4, long long nq, const double *T_host,
+                      void *stream);
+
 /* Size of the fixed device array qx_compute_2e_int_noalloc works in. */
 #define QX_NOALLOC_SCRATCH_BYTES (16u << 20)
 

@@ -6,13 +6,16 @@ real-solid-harmonic functions.  Every quantity is the Cartesian one transformed
 with the block-diagonal matrix T (n_sph x n_cart) of the shells' solid
 harmonics:
 
-    G_sph = (T x T x T x T) G_cart          four quarter transforms (batched GEMMs)
+    G_sph = (T x T x T x T) G_cart          dense tensor: four quarter transforms
+                                            (batched GEMMs); unique blocks: one
+                                            device kernel per class (qx_cart2sph_block)
     J, K  = T J_cart(T^T D T) T^T,  ...      (J and K are linear in D)
     grad  = grad_cart(T^T D T)              (Gamma built from D factorises)
     S, T, V = T M T^T
 
-so the kernels stay Cartesian and the transforms are dense FP64 matrix products
-(cuBLAS DGEMM; FP64 tensor cores on B200).
+so the kernels stay Cartesian and the transforms are FP64 matrix products
+(cuBLAS DGEMM, FP64 tensor cores on B200) or, for the unique blocks, a sparse
+transform kernel of this library.
 
 Conventions: Cartesian components in Libint's order, normalised so that x^l has
 unit norm; spherical functions in Libint's standard order m = -l..l, each of unit
@@ -20,12 +23,14 @@ norm (for l = 1: y, z, x).
 """
 from __future__ import annotations
 
+import ctypes as C
 import math
 
 import numpy as np
 import torch
 
 from ..basis import Basis, cart_components
+from . import _lib
 from .engine import EriEngine
 
 
@@ -81,6 +86,11 @@ def cart2sph(l: int) -> np.ndarray:
     return M
 
 
+# T_l for l = 0..3, row-major and concatenated: the coefficient table of the
+# device transform (qx_cart2sph_block)
+_T_PACKED = np.ascontiguousarray(np.concatenate([cart2sph(l).reshape(-1) for l in range(4)]))
+
+
 def transform_matrix(basis: Basis) -> np.ndarray:
     """Block-diagonal T (n_sph, n_cart) of a basis."""
     blocks = [cart2sph(s.l) for s in basis.shells]
@@ -116,6 +126,7 @@ class SphericalEngine:
         self.nbf = self.T.shape[0]
         self.natom = self.cart.natom
         self.basis = basis
+        self._unique = None  # (class info, Cartesian and spherical unique buffers)
 
     def close(self):
         self.cart.close()
@@ -140,7 +151,40 @@ class SphericalEngine:
     def eri_unique(self):
         """Per class, the spherical blocks of the screened unique quartets:
         {(la,lb,lc,ld): (s_a, s_b, s_c, s_d, nq) tensor} -- the Cartesian unique
-        layout transformed class by class with batched GEMMs."""
+        layout transformed class by class on the device (qx_cart2sph_block: one
+        thread per spherical value, the non-zero solid-harmonic coefficients
+        only), into one buffer kept between calls: the returned views hold the
+        latest call's values."""
+        if self._unique is None:
+            info = [c for c in self.cart.class_info()]
+            out_c = torch.empty(self.cart.unique_size(), dtype=torch.float64, device=self.device)
+            nsph = sum(int(np.prod([2 * l + 1 for l in c["l"]])) * c["nq"] for c in info)
+            out_s = torch.empty(max(nsph, 1), dtype=torch.float64, device=self.device)
+            self._unique = (info, out_c, out_s)
+        info, out_c, out_s = self._unique
+        self.cart.eri_unique(out_c)
+        lib = _lib.load()
+        stream = C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+        res, base, base_s = {}, 0, 0
+        for c in info:
+            l4 = tuple(c["l"])
+            size = int(np.prod([(l + 1) * (l + 2) // 2 for l in l4])) * c["nq"]
+            dims_s = [2 * l + 1 for l in l4]
+            size_s = int(np.prod(dims_s)) * c["nq"]
+            if c["nq"]:
+                la = np.array(l4, dtype=np.int32)
+                with torch.cuda.device(self.device):
+                    _lib.check(lib.qx_cart2sph_block(C.c_void_p(out_c[base:].data_ptr()),
+                                                     C.c_void_p(out_s[base_s:].data_ptr()), _lib.iptr(la),
+                                                     c["nq"], _lib.dptr(_T_PACKED), stream), "qx_cart2sph_block")
+                res[l4] = out_s[base_s:base_s + size_s].view(*dims_s, c["nq"])
+            base += size
+            base_s += size_s
+        return res
+
+    def eri_unique_gemm(self):
+        """eri_unique through four batched-GEMM quarter transforms per class
+        (torch/cuBLAS); the check on the device transform."""
         out_c = torch.empty(self.cart.unique_size(), dtype=torch.float64, device=self.device)
         self.cart.eri_unique(out_c)
         res, base = {}, 0

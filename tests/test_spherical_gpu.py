@@ -69,3 +69,39 @@ def test_spherical_gradient_finite_differences():
         Xm[nu] -= h
         fd = (energy(Xp) - energy(Xm)) / (2 * h)
         assert abs(fd - g[nu]) < 1e-6 * max(1.0, abs(fd))
+
+
+@pytest.mark.parametrize("f_shell", [False, True])
+def test_spherical_unique_blocks_device_transform(f_shell):
+    """The device transform of the unique blocks (qx_cart2sph_block, sparse
+    coefficients, one thread per value) against four batched-GEMM quarter
+    transforms of the same Cartesian blocks (1e-13: two FP64 summation orders),
+    on two calls in a row (its buffers are reused), with d and f shells."""
+    from quax_b200.integrals.spherical import SphericalEngine
+
+    spec = SyntheticSpec(natom=3, box=5.0, min_sep=1.2, kmax=3, exp_lo=0.1, exp_hi=50.0, f_shell=f_shell)
+    _, bc = synthetic_molecule(spec, 4)
+    eng = SphericalEngine(Basis(bc.shells, bc.natom, True, bc.name), 1e-12)
+    ref = eng.eri_unique_gemm()
+    assert not f_shell or any(3 in k for k in ref)
+    for _ in range(2):
+        got = eng.eri_unique()
+        assert got.keys() == ref.keys()
+        for k in ref:
+            assert got[k].shape == ref[k].shape
+            assert (got[k] - ref[k]).abs().max().item() < 1e-13, k
+    eng.close()
+
+
+def test_cart2sph_block_errors():
+    import ctypes as C
+
+    from quax_b200.integrals import _lib
+    from quax_b200.integrals.spherical import _T_PACKED
+
+    lib = _lib.load()
+    x = torch.zeros(8, dtype=torch.float64, device="cuda")
+    p = C.c_void_p(x.data_ptr())
+    for l4, nq, rc in (((4, 0, 0, 0), 1, -3), ((0, 0, 0, 0), -1, -1), ((1, 0, 0, 0), 0, 0)):
+        assert lib.qx_cart2sph_block(p, p, _lib.iptr(np.array(l4, dtype=np.int32)), nq, _lib.dptr(_T_PACKED),
+                                     None) == rc
