@@ -560,6 +560,15 @@ def gradient_60_atoms(S=128):
         r[k.replace("_s", "_s_estimate")] = a[k] * S
     r["adjoint_speedup_vs_plain"] = a["adjoint_speedup_vs_plain"]
     r["max_abs_diff_adjoint_vs_plain_Eh_per_bohr (shard)"] = a["max_abs_diff_adjoint_vs_plain_Eh_per_bohr"]
+    # one Hessian column (the JVP of the adjoint gradient along atom 0's x): only
+    # the quartets with a centre on atom 0 contribute, a few per cent of each
+    # list, so it is timed on a larger sample (1/16) than the gradient
+    S2 = 16
+    eng.set_shard(S2 // 2, S2)
+    v = torch.zeros(3 * eng.natom, dtype=torch.float64, device="cuda")
+    v[0] = 1.0
+    r["hessian_column_jvp_s_estimate"] = _time_ms(lambda: eng.grad_adjoint_jvp(D, v), 1, False) * 1e-3 * S2
+    r["hessian_column_sample"] = f"rank {S2 // 2} of {S2} cost-balanced shards; time x {S2}"
     eng.close()
     return r
 

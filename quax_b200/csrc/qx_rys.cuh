@@ -925,9 +925,15 @@ __global__ void __launch_bounds__(RysCls<LA, LB, LC, LD, KIND>::BS, RysCls<LA, L
         }
         double w9[9];
         if constexpr (KIND == RK_HVP) {
+            bool still = true;
 #pragma unroll
-            for (int b = 0; b < 9; ++b)
+            for (int b = 0; b < 9; ++b) {
                 w9[b] = __ldg(ra.dir + 3 * atoms[b / 3] + b % 3) - __ldg(ra.dir + 3 * atoms[3] + b % 3);
+                still = still && w9[b] == 0.0;
+            }
+            // the four atoms move alike along the direction: every term is linear
+            // in w, so the quartet adds nothing (team-uniform: one quartet per team)
+            if (still) continue;
         }
         const int nk = Q.nprim, ntot = P.nprim * nk;
         if constexpr (KIND == RK_PLAIN) {

@@ -285,6 +285,18 @@ __global__ void __launch_bounds__(WARP_QPB * 32) k_warp(WarpArgs wa, int mode) {
             if ((atA != a1 && atB != a1 && atC != a1 && atD != a1) || (atA != a2 && atB != a2 && atC != a2 && atD != a2))
                 return;
         }
+        if (DERIV == 2 && mode == WMODE_HVP) {
+            // a quartet whose four atoms move alike along v (w_X = v(X) - v(D) = 0
+            // for X = A, B, C) adds nothing: every term is linear in w.  For a
+            // Hessian column (v on one atom) that is every quartet off that atom.
+            bool still = true;
+            for (int x = 0; x < 3; ++x) {
+                const double vD = __ldg(wa.dir + 3 * atD + x);
+                still = still && __ldg(wa.dir + 3 * atA + x) == vD && __ldg(wa.dir + 3 * atB + x) == vD &&
+                        __ldg(wa.dir + 3 * atC + x) == vD;
+            }
+            if (still) return;  // whole warp (whole block when wpq = 4): one quartet
+        }
     }
     if (wa.acc_in) {
         const double* __restrict__ src = wa.acc_in + (size_t)qi * W::NITEM_PAD;
