@@ -615,6 +615,51 @@ def batched_extras(count: int, iterations: int = 20):
             "max_abs_gradient": float(max(abs(g).max() for g in G))}
 
 
+def config4_run(args):
+    """The batched uneven workload: `--config4` molecules (64 by default) of 3-40
+    atoms (sizes drawn from seed 0, molecule i generated with seed i), each with
+    FP64 RHF for 20 iterations -- every iteration's J/K of the whole batch
+    replayed from one CUDA graph, incremental density-screened builds with a full
+    rebuild every 8 iterations -- then the adjoint gradients.  Prints one JSON line."""
+    import numpy as np
+    import torch
+
+    from quax_b200.basis import SyntheticSpec, synthetic_molecule
+    from quax_b200.methods.batch import BatchedRHF
+
+    sizes = np.random.default_rng(0).integers(3, 41, size=args.config4)
+    mols, bases = [], []
+    for i, k in enumerate(sizes):
+        m, b = synthetic_molecule(SyntheticSpec(natom=int(k)), i)
+        mols.append(m)
+        bases.append(b)
+    t0 = time.perf_counter()
+    br = BatchedRHF(mols, bases, ints_tol=THR, incremental=1e-12, rebuild_every=8)
+    nq = sum(m.eng.unique_quartets() for m in br.mols)
+    br._jk_all()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    br._jk_all()
+    e1.record()
+    torch.cuda.synchronize()
+    jk_ms = e0.elapsed_time(e1)
+    t1 = time.perf_counter()
+    E, t_jk = br.scf(iterations=20, use_graph=True)
+    t2 = time.perf_counter()
+    G = br.gradients()
+    torch.cuda.synchronize()
+    t3 = time.perf_counter()
+    br.close()
+    print(json.dumps({"workload": f"{len(sizes)} molecules of 3-40 atoms (l<=2, Cartesian), FP64 RHF 20 iterations "
+                                  "+ adjoint gradients", "natoms": [int(k) for k in sizes],
+                      "nbf_total": int(sum(b.nbf() for b in bases)), "unique_quartets_per_full_jk": nq,
+                      "setup_s": t1 - t0, "full_jk_eager_ms": jk_ms, "full_jk_quartets_per_s": nq / (jk_ms * 1e-3),
+                      "scf_s": t2 - t1, "jk_graph_ms_per_iteration (incremental, density-screened builds)":
+                      t_jk / 20 * 1e3, "gradients_s": t3 - t2,
+                      "max_abs_gradient": float(max(abs(g).max() for g in G))}), flush=True)
+
+
 def run_grad_only(args):
     """Adjoint gradient of the workload only (profiling aid; prints its timing).
     With --profile-f: an 8-atom synthetic molecule with f shells on the heavy
@@ -717,6 +762,8 @@ def main():
                     help="displaced geometries in the batched-RHF extra (the full workload is 256)")
     ap.add_argument("--profile-grad", action="store_true",
                     help="run only the adjoint gradient of the workload, warmup+steps times (for profiler runs)")
+    ap.add_argument("--config4", type=int, default=0,
+                    help="run only the batched uneven workload with this many molecules (64: the full one)")
     ap.add_argument("--profile-f", action="store_true",
                     help="with --profile-grad: an 8-atom molecule with f shells instead of the workload")
     ap.add_argument("--no-extras", action="store_true",
@@ -728,6 +775,8 @@ def main():
         run_reference(args)
     elif args.profile_grad:
         run_grad_only(args)
+    elif args.config4:
+        config4_run(args)
     else:
         run_ours(args)
 

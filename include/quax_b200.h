@@ -240,6 +240,13 @@ int qx_set_engine(qx_handle *h, int cls, int plain, int pparam, int deriv, int d
  * without faulting the GPU. */
 int qx_set_wait_limit(qx_handle *h, int polls);
 
+/* Frees the first-derivative accumulators of the split-mode classes that a
+ * handle keeps after its first derivative call (up to 512 MiB per class; the
+ * next derivative call allocates them again).  No counterpart in the reference;
+ * for callers that hold many handles on one device (batched SCF).  Synchronises
+ * the device. */
+int qx_release_scratch(qx_handle *h);
+
 /* The canonical shell indices (s1, s2, s3, s4) of one class's screened unique
  * quartets, in the order of the unique layout (shells[4*qi + i], host memory of
  * 4 * nquartets ints).  No counterpart in the reference; lets a caller map the

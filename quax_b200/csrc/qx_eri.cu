@@ -1676,6 +1676,20 @@ extern "C" int qx_set_engine(qx_handle* h, int cls, int plain, int pparam, int d
     return QX_OK;
 }
 
+// Frees the first-derivative split-mode accumulators the handle keeps between
+// calls (the next derivative call of the class allocates them again), for
+// callers that hold many handles on one device.
+extern "C" int qx_release_scratch(qx_handle* h) {
+    if (!h) return fail(QX_E_INVALID, "qx_release_scratch: bad handle");
+    DeviceGuard g(h->device);
+    QX_CUDA(cudaDeviceSynchronize());  // no kernel of the handle still uses them
+    for (int c = 0; c < QX_NCLS_ALL; ++c) {
+        cudaFree(h->work[c].d_dacc);
+        h->work[c].d_dacc = nullptr;
+    }
+    return QX_OK;
+}
+
 // Polls of the bounded waits on the split-mode staging copies (default 4M); a
 // wait that runs out sets the error word, which host-synchronising calls report
 // as QX_E_DEVICE.  A limit of 0 makes every such wait run out (failure-path tests).

@@ -71,6 +71,7 @@ SIGNATURES = {
     "qx_gamma_tile": (C.c_int, [_vp, C.c_int, C.c_longlong, C.c_longlong, C.c_int, _vp, C.c_double, C.c_double, _vp,
                                 _vp]),
     "qx_cart2sph_block": (C.c_int, [_vp, _vp, _ip, C.c_longlong, _dp, _vp]),
+    "qx_release_scratch": (C.c_int, [_vp]),
     "qx_compute_2e_int_noalloc": (
         C.c_int,
         [C.c_int, _dp, C.c_int, _ip, _ip, _ip, _dp, _dp, C.c_double, _vp, _vp],

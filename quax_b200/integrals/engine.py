@@ -221,6 +221,12 @@ class EriEngine:
             _lib.check(_lib.load().qx_set_engine(self.handle, int(cls), pe, int(plain_param), de, int(deriv_param)),
                        "qx_set_engine")
 
+    def release_scratch(self) -> None:
+        """Free the derivative accumulators the handle keeps between calls (for
+        many handles on one device; the next derivative call allocates again)."""
+        with torch.cuda.device(self.device):
+            _lib.check(_lib.load().qx_release_scratch(self.handle), "qx_release_scratch")
+
     def set_wait_limit(self, polls: int) -> None:
         """Polls of the bounded waits on the split-mode staging copies (0 makes
         them run out: the host-synchronising calls then raise QuaxError)."""

@@ -199,6 +199,7 @@ class BatchedRHF:
             g = g + m.eng.grad_adjoint(D, 2.0, -1.0)
             out.append(g.cpu().numpy() + nuclear_repulsion(m.mol.Z, m.mol.coords, deriv=True)[1])
             del dS, dT, dV
+            m.eng.release_scratch()  # one molecule's derivative accumulators at a time
         return out
 
     def close(self):

@@ -79,3 +79,24 @@ def test_bounded_wait_timeout_reports_device_error(oracle_lib):
     G = eng.eri_host().reshape(eng.nbf, eng.nbf, eng.nbf, eng.nbf)
     ref = oracle_lib.compute_2e_int(oracle_lib.OracleBasis(b), 1e-12)
     assert np.abs(G - ref).max() < 1e-12
+
+
+def test_release_scratch_then_gradient_again():
+    """qx_release_scratch frees the cached derivative accumulators; the next
+    gradient allocates them again and gives the same result (1e-12)."""
+    import torch
+
+    from quax_b200.integrals.engine import EriEngine
+
+    spec = SyntheticSpec(natom=3, box=5.0, min_sep=1.2, kmax=4, exp_lo=0.1, exp_hi=50.0)
+    b = synthetic_molecule(spec, 3)[1]
+    eng = EriEngine(b, 1e-12)
+    n = eng.nbf
+    C = np.random.default_rng(0).normal(0.0, 1.0 / np.sqrt(n), size=(n, n // 4))
+    D = torch.from_numpy(C @ C.T).cuda()
+    g1 = eng.grad_adjoint(D).cpu().numpy()
+    eng.release_scratch()
+    eng.release_scratch()  # twice: nothing left to free
+    g2 = eng.grad_adjoint(D).cpu().numpy()
+    assert np.abs(g1 - g2).max() < 1e-12
+    eng.close()
