@@ -473,7 +473,7 @@ def _hessian_column(eng, D, warm=True):
 
 
 def gradient_headline(eng10, b10, oracle_check=True):
-    """The north-star quantity: s per evaluation of the HF-type gradient
+    """The headline quantity: s per evaluation of the HF-type gradient
     sum Gamma_ijkl d(ij|kl)/dR (Gamma = D_ij D_kl - 1/2 D_ik D_jl), adjoint kernel
     vs the plain FP64 derivative-tensor path, on the 10- and 30-atom workloads in
     full and on the 60-atom workload with f shells through a cost-balanced shard."""

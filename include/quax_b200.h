@@ -40,7 +40,7 @@ extern "C" {
 #define QX_E_NOMEM (-4)       /* device allocation failed */
 #define QX_E_DEVICE (-5)      /* a kernel reported an error through the error word */
 
-/* Highest angular momentum per shell compiled into this build (f shells). */
+/* Highest angular momentum per shell the library is compiled for (f shells). */
 #define QX_MAX_L 3
 
 typedef struct qx_handle qx_handle;

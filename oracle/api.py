@@ -1,7 +1,8 @@
 """ctypes front-end of the CPU FP64 oracle (oracle/eri_oracle.c).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
-CPU legs of bench.py as the checker; never by the product package.
+CPU legs of bench.py, as the reference results to compare with; never by the
+product package.
 """
 from __future__ import annotations
 

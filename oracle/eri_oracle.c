@@ -2,8 +2,8 @@
  * eri_oracle.c -- CPU FP64 oracle for the two-electron integral path.
  *
  * TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and bench.py's
- * cpu_baseline / reference legs may load this library, and only as the checker
- * (or the timed CPU arm).  The product path never calls it.
+ * cpu_baseline / reference legs may load this library, and only as the results to
+ * compare with (or the timed CPU arm).  The product path never calls it.
  *
  * What it restates:
  *   - Schwarz screening with the reference's semantics

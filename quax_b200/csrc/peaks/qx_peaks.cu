@@ -1,7 +1,7 @@
 // qx_peaks.cu -- FP64 / FP32 FMA throughput probe (libqx_peaks.so).
 //
 // The roofline denominator for the FP64 integral kernels: the measured peaks the
-// benchmark driver provides cover HBM bandwidth and bf16 tensor throughput only,
+// machine provides cover HBM bandwidth and bf16 tensor throughput only,
 // so the FP64 and FP32 FMA peaks are measured here.  Every thread runs 8
 // independent FMA chains (enough to cover the pipe latency), the grid covers every
 // SM many times, and time comes from CUDA events around the launch.

@@ -1255,7 +1255,7 @@ static int run_all_derk(qx_handle* h, int k, double* out, const int* nu, cudaStr
 extern "C" int qx_eri_deriv_core(qx_handle* h, int order, double* out, int out_on_device, void* stream) {
     if (!h || !out) return fail(QX_E_INVALID, "qx_eri_deriv_core: NULL argument");
     if (order < 1 || order > 4)
-        return fail(QX_E_UNSUPPORTED, "qx_eri_deriv_core: derivative order %d (this build: 1 to 4)", order);
+        return fail(QX_E_UNSUPPORTED, "qx_eri_deriv_core: derivative order %d (this library: 1 to 4)", order);
     DeviceGuard g(h->device);
     cudaStream_t s = (cudaStream_t)stream;
     const long long n = h->nbf, n4 = n * n * n * n;
@@ -1283,7 +1283,7 @@ extern "C" int qx_compute_2e_deriv(qx_handle* h, const int* deriv_vec, int len, 
         order += deriv_vec[i];
     }
     if (order < 1 || order > 4)
-        return fail(QX_E_UNSUPPORTED, "qx_compute_2e_deriv: derivative order %d (this build: 1 to 4)", order);
+        return fail(QX_E_UNSUPPORTED, "qx_compute_2e_deriv: derivative order %d (this library: 1 to 4)", order);
     if (order == 2 && len > 0xffff) return fail(QX_E_INVALID, "qx_compute_2e_deriv: too many atoms for order 2");
     DeviceGuard g(h->device);
     cudaStream_t s = (cudaStream_t)stream;
@@ -1406,7 +1406,7 @@ extern "C" int qx_oei(qx_handle* h, double* S, double* T, double* V, void* strea
 
 extern "C" int qx_oei_deriv_core(qx_handle* h, int order, double* dS, double* dT, double* dV, void* stream) {
     if (!h || !dS || !dT || !dV) return fail(QX_E_INVALID, "qx_oei_deriv_core: NULL argument");
-    if (order != 1) return fail(QX_E_UNSUPPORTED, "qx_oei_deriv_core: derivative order %d (this build: 1)", order);
+    if (order != 1) return fail(QX_E_UNSUPPORTED, "qx_oei_deriv_core: derivative order %d (this library: 1)", order);
     if (!h->d_Z) return fail(QX_E_INVALID, "qx_oei_deriv_core: nuclear charges not set (qx_set_charges)");
     DeviceGuard g(h->device);
     cudaStream_t s = (cudaStream_t)stream;

@@ -26,7 +26,7 @@ def _stream_ptr(stream) -> int:
 class EriEngine:
     def __init__(self, basis: Basis, ints_tol: float = 1.0e-14, device=None):
         if basis.pure:
-            raise NotImplementedError("spherical shells are not supported by this build (Cartesian only)")
+            raise NotImplementedError("spherical shells are not supported by this engine (Cartesian only; see SphericalEngine)")
         lib = _lib.load()
         if not torch.cuda.is_available():
             raise _lib.QuaxError("no CUDA device: the ERI engine has no CPU path")

@@ -94,7 +94,7 @@ def compute_2e_deriv(type_: str, beta: float, deriv_vec) -> np.ndarray:
 def eri_deriv_core(deriv_order: int) -> np.ndarray:
     eng = _engine()
     if deriv_order > LIBINT2_MAX_DERIV_ORDER:
-        raise NotImplementedError(f"derivative order {deriv_order} (this build: {LIBINT2_MAX_DERIV_ORDER})")
+        raise NotImplementedError(f"derivative order {deriv_order} (this library: {LIBINT2_MAX_DERIV_ORDER})")
     out = eng.eri_deriv_core(deriv_order)
     assert out.shape[0] == how_many_derivs(eng.natom, deriv_order)
     return out.reshape(-1).cpu().numpy()
@@ -123,13 +123,13 @@ def compute_1e_deriv(type_: str, deriv_vec) -> np.ndarray:
     if order == 0:
         return compute_1e_int(type_)
     if order != 1 or (dv < 0).any():
-        raise NotImplementedError(f"one-electron derivative order {order} (this build: 1)")
+        raise NotImplementedError(f"one-electron derivative order {order} (this library: 1)")
     return eng.oei_deriv(1)[k][int(np.argmax(dv))].reshape(-1).cpu().numpy()
 
 
 def oei_deriv_core(deriv_order: int):
     if deriv_order != 1:
-        raise NotImplementedError(f"one-electron derivative order {deriv_order} (this build: 1)")
+        raise NotImplementedError(f"one-electron derivative order {deriv_order} (this library: 1)")
     return [x.reshape(-1).cpu().numpy() for x in _engine().oei_deriv(1)]
 
 
@@ -186,7 +186,7 @@ def compute_2e_deriv_disk(type_: str, beta: float, max_deriv_order: int) -> str:
     if n**4 * slices * 8e-9 >= _DISK_LIMIT_GB:
         raise ValueError(f"ERI derivative tensors need {n**4 * slices * 8e-9:.0f} GB (limit {_DISK_LIMIT_GB:.0f} GB)")
     if max_deriv_order > LIBINT2_MAX_DERIV_ORDER:
-        raise NotImplementedError(f"derivative order {max_deriv_order} (this build: {LIBINT2_MAX_DERIV_ORDER})")
+        raise NotImplementedError(f"derivative order {max_deriv_order} (this library: {LIBINT2_MAX_DERIV_ORDER})")
     data = {}
     for k in range(1, max_deriv_order + 1):
         d = eng.eri_deriv_core(k).cpu().numpy()
@@ -196,7 +196,7 @@ def compute_2e_deriv_disk(type_: str, beta: float, max_deriv_order: int) -> str:
 
 def compute_1e_deriv_disk(type_: str, max_deriv_order: int) -> str:
     """Write one-electron derivative tensors to oei_derivs.(h5|npz): datasets
-    <type>_<n>_<n>_deriv<k>, shape (n, n, nderiv); first order in this build."""
+    <type>_<n>_<n>_deriv<k>, shape (n, n, nderiv); first order in this library."""
     return _oei_disk([type_], max_deriv_order)
 
 
@@ -208,7 +208,7 @@ def oei_deriv_disk(max_deriv_order: int) -> str:
 def _oei_disk(types, max_deriv_order: int) -> str:
     ks = [_oei_index(t) for t in types]
     if max_deriv_order != 1:
-        raise NotImplementedError(f"one-electron derivative order {max_deriv_order} (this build: 1)")
+        raise NotImplementedError(f"one-electron derivative order {max_deriv_order} (this library: 1)")
     eng = _engine()
     n = eng.nbf
     d = eng.oei_deriv(1)

@@ -91,7 +91,7 @@ class TEI:
             # tei.py:29-34: one tensor of unique derivatives per order
             top = _lib.load().qx_max_deriv_order()
             if max_deriv_order > top:
-                raise NotImplementedError(f"precomputed derivative tensors of order {max_deriv_order} (this build: {top})")
+                raise NotImplementedError(f"precomputed derivative tensors of order {max_deriv_order} (this library: {top})")
             for k in range(1, max_deriv_order + 1):
                 d = self.engine.eri_deriv_core(k)
                 assert d.shape[0] == how_many_derivs(self.natom, k)
