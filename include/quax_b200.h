@@ -129,8 +129,10 @@ int qx_grad_adjoint(qx_handle *h, const double *D, double cj, double ck, double 
  * of quax/methods/hartree_fock.py:26-28,79-80,92-93 (J = jk_build(G, D),
  * K = jk_build(G.transpose(0,2,1,3), D)) without forming G:
  *     J_ij = sum_kl (ij|kl) D_kl,   K_ij = sum_kl (ik|jl) D_kl      (n x n, row-major)
- * over the screened unique quartets.  J and K are overwritten; D, J, K are device
- * pointers when on_device = 1, host pointers otherwise. */
+ * over the screened unique quartets, for a symmetric D (the densities of an SCF;
+ * the images of each integral are folded with D_kl = D_lk).  J and K are
+ * overwritten; D, J, K are device pointers when on_device = 1, host pointers
+ * otherwise. */
 int qx_jk(qx_handle *h, const double *D, double *J, double *K, int on_device, void *stream);
 
 /* Angular-momentum classes (canonical (la lb|lc ld), la>=lb, lc>=ld, bra class >=

@@ -78,9 +78,16 @@ def test_f_schwarz_and_unique_blocks(oracle_lib):
     assert nq == eng.unique_quartets() == oracle_lib.count_unique(ob, 1e-12)
 
 
-def test_f_jk(oracle_lib):
+@pytest.mark.parametrize("all_rys", [False, True])
+def test_f_jk(oracle_lib, all_rys):
+    """Direct J/K with f shells (the Rys engine's block-contraction epilogue),
+    with the default engines and with the Rys engine on every class, against the
+    oracle's dense tensor contracted with D (1e-10)."""
     b = f_synthetic(3)
     eng = _engine(b, 1e-12)
+    if all_rys:
+        for c in eng.class_info():
+            eng.set_engine(c["cls"], plain="rys")
     n = eng.nbf
     D = density(n, 3)
     J, Kx = eng.jk(torch.from_numpy(D).cuda())
