@@ -3,9 +3,10 @@
 // The device kernel runs the same functions (qx_rys.cuh: rys_prim, rys_fn, the
 // table builders and the product steps) over a team of threads; here one host
 // thread runs them with (tid, nth) = (0, 1), so tests on a machine without a GPU
-// can compare the engine's arithmetic with the oracle: plain integrals and the
-// nine first-derivative sums of the adjoint gradient, with either table build and
-// with the root batching of the compiled kernel.
+// can compare the engine's arithmetic with the oracle: plain integrals, the nine
+// first-derivative sums of the adjoint gradient, the Hessian-vector sums and the
+// derivative blocks of orders 1 and 2, with either table build and with the root
+// batching of the compiled kernel.
 #include <cmath>
 #include <vector>
 
@@ -56,14 +57,25 @@ void make_pair(const Sh& a, const Sh& b, PairInfo& P, std::vector<PrimPair>& pr)
 // build: 0 level-parallel tables, 1 per-unit tables, 2 as the compiled kernel
 // (its per-unit/level-parallel choice and its RB-root batches).
 template <int LA, int LB, int LC, int LD, int KIND>
-void run(const Sh* s, const double* gam, int build, double* out) {
+void run(const Sh* s, const double* gam, const double* w9, int build, double* out) {
     using C = RysCls<LA, LB, LC, LD, KIND>;
     PairInfo P, Q;
     std::vector<PrimPair> pp, qq;
     make_pair(s[0], s[1], P, pp);
     make_pair(s[2], s[3], Q, qq);
-    std::vector<double> uw(2 * C::NR), U((size_t)C::NR * 3 * C::USZ);
-    std::vector<double> acc(C::NCOMP, 0.0);
+    std::vector<double> uw(2 * C::NR), U((size_t)C::NR * 3 * C::USZ), O((size_t)C::NR * 3 * (C::UOPS + 1));
+    // derivative tensors: every multi-index of the quartet's 12 centre-directions
+    const int nmulti = KIND >= RK_DER1 ? rys_binom(12 + C::K::ORD - 1, C::K::ORD) : 1;
+    std::vector<int> mops(nmulti, 0);
+    if constexpr (KIND >= RK_DER1) {
+        const int atoms[4] = {0, 1, 2, 3};
+        for (int m = 0; m < nmulti; ++m) {
+            long long slot;
+            double mult;
+            rys_derk_index(C::K::ORD, m, atoms, 12, nullptr, 0, mops[m], slot, mult);
+        }
+    }
+    std::vector<double> acc((size_t)C::NCOMP * nmulti, 0.0);
     double g[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     const int rb = build == 2 ? C::RB : C::NR;
     const bool seq = build == 1 || (build == 2 && C::SEQ);
@@ -81,19 +93,25 @@ void run(const Sh* s, const double* gam, int build, double* out) {
                     for (int b = 1; b < C::B1; ++b) rys_phase_bra<C>(st, b, nrb, U.data(), 0, 1);
                     for (int d = 0; d < C::D1; ++d) rys_phase_ket<C>(st, d, nrb, U.data(), 0, 1);
                 }
+                if constexpr (C::NOPS > 0) rys_phase_ops<C, KIND, LA, LB, LC, LD>(st, nrb, U.data(), O.data(), w9, 0, 1);
                 for (int kc = 0; kc < C::NCOMP; ++kc) {
                     const int off = rys_comp_offsets<C, LA, LB, LC, LD, C::RAW>(kc);
                     if constexpr (KIND == RK_PLAIN)
                         acc[kc] += rys_prod_plain<C>(U.data(), nrb, off);
-                    else
+                    else if constexpr (KIND == RK_GRAD)
                         rys_prod_grad<C>(U.data(), nrb, off, rys_comp_exps<C, LA, LB, LC, LD>(kc), st.e2, gam[kc], g);
+                    else if constexpr (KIND == RK_HVP)
+                        rys_prod_hvp<C>(O.data(), nrb, off, gam[kc], g);
+                    else
+                        for (int m = 0; m < nmulti; ++m)
+                            acc[(size_t)m * C::NCOMP + kc] += rys_prod_derk<C>(O.data(), nrb, off, mops[m]);
                 }
             }
         }
-    if constexpr (KIND == RK_PLAIN)
-        for (int kc = 0; kc < C::NCOMP; ++kc) out[kc] = acc[kc];
-    else
+    if constexpr (KIND == RK_GRAD || KIND == RK_HVP)
         for (int b = 0; b < 9; ++b) out[b] = g[b];
+    else
+        for (size_t i = 0; i < acc.size(); ++i) out[i] = acc[i];
 }
 
 }  // namespace
@@ -108,12 +126,16 @@ extern "C" void rys_host_class(int i, int* l4) {
     for (int k = 0; k < 4; ++k) l4[k] = kL[i][k];
 }
 
-// kind 0: plain block (NCOMP values), 1: the nine sums g[3X + x] = sum_kc gam_kc
-// d/dX_x (ab|cd)_kc, X = A, B, C.  Shells: centres cen[12], primitive counts
+// kind 0: plain block (NCOMP values); 1: the nine sums g[3X + x] = sum_kc gam_kc
+// d/dX_x (ab|cd)_kc, X = A, B, C; 2: the Hessian-vector sums h[3X + x] = sum_kc
+// gam_kc sum_V w9[V] d2/dX_x dV (ab|cd)_kc; 11, 12: the derivative blocks of
+// orders 1 and 2, one NCOMP block per sorted multi-index of the 12
+// centre-directions 3 * centre + xyz.  Shells: centres cen[12], primitive counts
 // np[4], exponents and normalised coefficients concatenated.
 extern "C" int rys_host(int kind, int cls, int build, const double* cen, const int* np, const double* exps,
-                        const double* wts, const double* gam, double* out) {
-    if (cls < 0 || cls >= rys_host_nclass() || kind < 0 || kind > 1 || build < 0 || build > 2) return -1;
+                        const double* wts, const double* gam, const double* w9, double* out) {
+    if (cls < 0 || cls >= rys_host_nclass() || build < 0 || build > 2) return -1;
+    if (kind != 0 && kind != 1 && kind != 2 && kind != 11 && kind != 12) return -1;
     Sh s[4];
     int o = 0;
     for (int c = 0; c < 4; ++c) {
@@ -124,12 +146,13 @@ extern "C" int rys_host(int kind, int cls, int build, const double* cen, const i
         s[c].w = wts + o;
         o += np[c];
     }
-#define QX_HOST_CASE(i, a, b, c, d)                                  \
-    case i:                                                          \
-        if (kind == 0)                                               \
-            run<a, b, c, d, RK_PLAIN>(s, gam, build, out);           \
-        else                                                         \
-            run<a, b, c, d, RK_GRAD>(s, gam, build, out);            \
+#define QX_HOST_CASE(i, a, b, c, d)                                                   \
+    case i:                                                                           \
+        if (kind == 0) run<a, b, c, d, RK_PLAIN>(s, gam, w9, build, out);             \
+        if (kind == 1) run<a, b, c, d, RK_GRAD>(s, gam, w9, build, out);              \
+        if (kind == 2) run<a, b, c, d, RK_HVP>(s, gam, w9, build, out);               \
+        if (kind == 11) run<a, b, c, d, RK_DER1>(s, gam, w9, build, out);             \
+        if (kind == 12) run<a, b, c, d, RK_DER2>(s, gam, w9, build, out);             \
         return 0;
     switch (cls) {
         QX_HOST_CASE(0, 0, 0, 0, 0)
